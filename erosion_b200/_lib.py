@@ -1,0 +1,168 @@
+"""ctypes binding of the C ABI in ``include/erosion_b200.h``.
+
+The library ``libstokes_b200.so`` is built in-tree (``erosion_b200/build.py``).
+There is no CPU fallback: every function here raises if the shared library is
+missing, and the library itself reports EROSION_NO_DEVICE when no CUDA device
+is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libstokes_b200.so")
+
+EROSION_OK = 0
+EROSION_MAXITER = 1
+EROSION_BREAKDOWN = 2
+EROSION_BAD_INPUT = 3
+EROSION_CUDA_ERROR = 4
+EROSION_NO_DEVICE = 5
+
+STATUS_NAMES = {
+    EROSION_OK: "ok",
+    EROSION_MAXITER: "maxiter",
+    EROSION_BREAKDOWN: "breakdown",
+    EROSION_BAD_INPUT: "bad_input",
+    EROSION_CUDA_ERROR: "cuda_error",
+    EROSION_NO_DEVICE: "no_device",
+}
+
+PD = POINTER(c_double)
+PI64 = POINTER(c_int64)
+
+
+class ErosionParams(ctypes.Structure):
+    """Mirror of ``erosion_params``."""
+
+    _fields_ = [
+        ("wall_a", c_double),
+        ("wall_b", c_double),
+        ("wall_order", c_double),
+        ("tol", c_double),
+        ("maxl", c_int64),
+        ("ibary", c_int32),
+        ("ifmm", c_int32),
+        ("ibc", c_int32),
+        ("precision", c_int32),
+        ("rhs_mode", c_int32),
+        ("true_residual", c_int32),
+        ("reserved", c_int32 * 6),
+    ]
+
+
+class SolveStats(ctypes.Structure):
+    """Mirror of ``erosion_solve_stats``."""
+
+    _fields_ = [
+        ("iterations", c_int64),
+        ("matvecs", c_int64),
+        ("matvecs_fp32", c_int64),
+        ("sweeps", c_int64),
+        ("est_residual", c_double),
+        ("true_residual", c_double),
+        ("ms_total", c_double),
+        ("ms_far", c_double),
+        ("far_launches", c_int64),
+        ("near_pairs", c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every entry point declared in include/erosion_b200.h, with its signature.
+SIGNATURES = {
+    "stokessolver_": (None, [PI64] * 7 + [PD, PD, PD, PI64]),
+    "computeshearstress_": (None, [PI64, PI64, PI64, PD, PD, PD, PI64, PD]),
+    "computeqoitargets_": (None, [PI64, PI64, PI64, PI64, PD, PD, PD, PI64, PD, PD, PD, PD, PD, PD]),
+    "erosion_last_status": (c_int, []),
+    "erosion_last_error": (c_char_p, []),
+    "erosion_default_params": (None, [POINTER(ErosionParams)]),
+    "erosion_solve": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PI64]),
+    "erosion_solve_device": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, PI64]),
+    "erosion_get_solve_stats": (None, [POINTER(SolveStats)]),
+    "erosion_matvec": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD]),
+    "erosion_rhs": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD]),
+    "erosion_geometry": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD] + [PD] * 12),
+    "erosion_shear_stress": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD, PD]),
+    "erosion_shear_stress_device": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "erosion_qoi_targets": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, c_int64,
+                                    PD, PD, PD, PD, PD, PD]),
+    "erosion_near_info": (c_int64, [PI64, PI64, PI64]),
+    "erosion_release": (None, []),
+}
+
+_lib = None
+
+
+class ErosionError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"{p} is missing: build it with `python -m erosion_b200.build` "
+                          "(the CUDA library has no CPU fallback)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        if not hasattr(lib, name):
+            continue    # reported by missing_symbols(); calling it raises AttributeError
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def missing_symbols(lib: ctypes.CDLL | None = None) -> list[str]:
+    lib = lib or load()
+    return [n for n in SIGNATURES if not hasattr(lib, n)]
+
+
+def ptr(a: np.ndarray) -> PD:
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(PD)
+
+
+def default_params(**kw) -> ErosionParams:
+    p = ErosionParams()
+    load().erosion_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if k in ("wall",):
+            p.wall_a, p.wall_b, p.wall_order = v
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def last_error() -> tuple[int, str]:
+    lib = load()
+    return lib.erosion_last_status(), (lib.erosion_last_error() or b"").decode()
+
+
+def check(rc: int, allow=(EROSION_OK,)) -> int:
+    if rc not in allow:
+        code, msg = last_error()
+        raise ErosionError(rc, msg)
+    return rc
+
+
+def solve_stats() -> dict:
+    s = SolveStats()
+    load().erosion_get_solve_stats(ctypes.byref(s))
+    return s.as_dict()

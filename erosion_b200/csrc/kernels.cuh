@@ -1,0 +1,652 @@
+// Device kernels of the boundary operator, its geometry and the Krylov
+// solver.  Launch wrappers live in solver.cu.
+#pragma once
+#include "common.cuh"
+
+// Internal linkage: the translation units that include this header each get
+// their own copy of the kernels they launch.
+namespace {
+
+// Problem-wide constants of the far-field kernels.
+constexpr int FAR_NT = 256;        // threads per CTA
+constexpr int FAR_TPT = 2;         // targets per thread (FP64)
+constexpr int FAR_TS = 256;        // sources per shared-memory tile (<= FAR_NT)
+constexpr int NEAR_NT = 128;       // threads per CTA of the barycentric kernels
+constexpr int NEAR_TK = 128;       // source nodes per shared-memory tile
+constexpr int BD_NT = 256;         // threads per CTA of the boundary-value kernel
+
+// ---------------------------------------------------------------------------
+// Geometry (stokesSolver.f:136-204, :417-457).
+
+// Wall nodes of the superellipse x = a r cos t, y = b r sin t,
+// r = (|cos t|^p + |sin t|^p)^(-1/p), t = k 2pi/nout (:182-191).
+__global__ void k_wall_nodes(int nout, double a, double b, double p, double* __restrict__ x,
+                             double* __restrict__ y) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nout) return;
+  double dth = EB_TWOPI / nout;
+  double th = k * dth;
+  double c = cos(th), s = sin(th);
+  double r = pow(pow(fabs(c), p) + pow(fabs(s), p), -1.0 / p);
+  x[k] = a * r * c;
+  y[k] = b * r * s;
+}
+
+// One CTA per curve of length n.  First and second spectral derivatives by
+// circulant convolution with dk[m] = (1/2)(-1)^m cot(pi m/n), the matrix of
+// fourierDiff (:348-388, even n); then speed, normal (-y', x')/|z'|,
+// curvature (y'x'' - x'y'')/|z'|^3 (:447-453), negated on the wall (:195-199).
+__global__ void k_geom(const double* __restrict__ x, const double* __restrict__ y, int n,
+                       const double* __restrict__ dk, int out_off, int negate,
+                       double2* __restrict__ xy, double2* __restrict__ nrm, double* __restrict__ sp,
+                       double* __restrict__ cur, double* __restrict__ w, double2* __restrict__ dz,
+                       double2* __restrict__ d1tmp) {
+  const int c = blockIdx.x;
+  const double* xc = x + (size_t)c * n;
+  const double* yc = y + (size_t)c * n;
+  double2* D1 = d1tmp + (size_t)c * n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double ax = 0.0, ay = 0.0;
+    for (int k = 0; k < n; ++k) {
+      int m = j - k;
+      if (m < 0) m += n;
+      double d = __ldg(dk + m);
+      ax = fma(d, __ldg(xc + k), ax);
+      ay = fma(d, __ldg(yc + k), ay);
+    }
+    D1[j] = make_double2(ax, ay);
+  }
+  __syncthreads();
+  const double h = EB_TWOPI / n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double bx = 0.0, by = 0.0;
+    for (int k = 0; k < n; ++k) {
+      int m = j - k;
+      if (m < 0) m += n;
+      double d = __ldg(dk + m);
+      double2 q = D1[k];
+      bx = fma(d, q.x, bx);
+      by = fma(d, q.y, by);
+    }
+    double2 q = D1[j];
+    double Dx = q.x, Dy = q.y, DDx = bx, DDy = by;
+    double s = sqrt(Dx * Dx + Dy * Dy);
+    double px = -Dy / s, py = Dx / s;
+    double cu = (Dy * DDx - Dx * DDy) / (s * s * s);
+    if (negate) { px = -px; py = -py; cu = -cu; }
+    int g = out_off + c * n + j;
+    xy[g] = make_double2(xc[j], yc[j]);
+    nrm[g] = make_double2(px, py);
+    sp[g] = s;
+    cur[g] = cu;
+    w[g] = s * h / EB_PI;
+    dz[g] = make_double2(Dx * h, Dy * h);
+  }
+}
+
+// Centroid (plain node mean, :151-160) and mean speed (the body radius of
+// matvec_DLP_fmmbary, :697-703) per body.
+__global__ void k_body_stats(int n, int nout, const double2* __restrict__ xy, const double* __restrict__ sp,
+                             double2* __restrict__ cen, double* __restrict__ rb) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x;
+  double sx = 0, sy = 0, ss = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    int g = nout + b * n + k;
+    sx += xy[g].x; sy += xy[g].y; ss += sp[g];
+  }
+  sx = block_sum<256>(sx, sh);
+  sy = block_sum<256>(sy, sh);
+  ss = block_sum<256>(ss, sh);
+  if (threadIdx.x == 0) { cen[b] = make_double2(sx / n, sy / n); rb[b] = ss / n; }
+}
+
+// ---------------------------------------------------------------------------
+// Per-matvec preparation: one CTA per curve.  Writes the weighted source
+// strengths w*sigma used by the far field, the constraint rows of every body
+// (:1055-1096) and the wall's integral of sigma.n for the rank-one term
+// (:1107-1111).
+__global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict__ den,
+                                              double2* __restrict__ ws, double* __restrict__ vel,
+                                              double* __restrict__ sigdotn) {
+  __shared__ double sh[32];
+  const int c = blockIdx.x;
+  const int start = curve_start(G, c), len = curve_len(G, c);
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int j = threadIdx.x; j < len; j += blockDim.x) {
+    int g = start + j;
+    double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+    double wg = G.w[g], s = G.sp[g];
+    ws[g] = make_double2(wg * sx, wg * sy);
+    if (c == 0) {
+      double2 nn = G.nrm[g];
+      a0 += (nn.x * sx + nn.y * sy) * s;
+    } else {
+      double2 p = G.xy[g];
+      a0 += sx * s;
+      a1 += sy * s;
+      a2 += (sx * p.y - sy * p.x) * s;
+    }
+  }
+  a0 = block_sum<256>(a0, sh);
+  if (c == 0) {
+    if (threadIdx.x == 0) *sigdotn = a0 * (EB_TWOPI / len);
+    return;
+  }
+  a1 = block_sum<256>(a1, sh);
+  a2 = block_sum<256>(a2, sh);
+  if (threadIdx.x == 0) {
+    int b = c - 1;
+    vel[ic_of(G, b, 0)] = (-a0) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 0)];
+    vel[ic_of(G, b, 1)] = (-a1) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 1)];
+    vel[ic_of(G, b, 2)] = (-a2) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 2)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Far field, FP64: u_i = sum_{j != i} (r.n_j)(r.w_j sigma_j)/rho^4 r,
+// r = x_i - x_j, over every node pair except the (target, source curve) pairs
+// that the near-field bookkeeping replaces (bit c of mask[i]).  This is the
+// sum the reference's FMM approximates (stokesSolver.f:636-680; direct form
+// :1563-1584).  Sources are staged tile by tile in shared memory; a tile never
+// crosses a curve, so the mask test is one bit per tile and target.  blockIdx.y
+// selects a contiguous range of tiles (split-K); partial sums are reduced in a
+// fixed order by k_combine.
+__device__ __forceinline__ double rcp_or_zero(double r2) { return r2 > 0.0 ? __drcp_rn(r2) : 0.0; }
+
+template <bool MASK>
+__global__ void __launch_bounds__(FAR_NT, 2)
+k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
+        const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
+        double2* __restrict__ partial) {
+  __shared__ double4 sg[FAR_TS];
+  __shared__ double2 sw[FAR_TS];
+  const int N = G.N;
+  const int split = blockIdx.y;
+  const int i0 = blockIdx.x * (FAR_NT * FAR_TPT) + threadIdx.x;
+  int it[FAR_TPT];
+  double px[FAR_TPT], py[FAR_TPT], ax[FAR_TPT], ay[FAR_TPT];
+#pragma unroll
+  for (int q = 0; q < FAR_TPT; ++q) {
+    int i = i0 + q * FAR_NT;
+    it[q] = i < N ? i : N - 1;
+    double2 p = G.xy[it[q]];
+    px[q] = p.x; py[q] = p.y; ax[q] = 0.0; ay[q] = 0.0;
+  }
+  const int tb = split_ptr[split], te = split_ptr[split + 1];
+  for (int ti = tb; ti < te; ++ti) {
+    const int4 T = tiles[ti];
+    __syncthreads();
+    if (threadIdx.x < T.y) {
+      int g = T.x + threadIdx.x;
+      double2 q = G.xy[g], nn = G.nrm[g];
+      sg[threadIdx.x] = make_double4(q.x, q.y, nn.x, nn.y);
+      sw[threadIdx.x] = ws[g];
+    }
+    __syncthreads();
+    double tx[FAR_TPT], ty[FAR_TPT];
+#pragma unroll
+    for (int q = 0; q < FAR_TPT; ++q) { tx[q] = 0.0; ty[q] = 0.0; }
+#pragma unroll 2
+    for (int j = 0; j < T.y; ++j) {
+      const double4 s = sg[j];
+      const double2 a = sw[j];
+#pragma unroll
+      for (int q = 0; q < FAR_TPT; ++q) {
+        double rx = px[q] - s.x, ry = py[q] - s.y;
+        double rho2 = fma(rx, rx, ry * ry);
+        double rdn = fma(rx, s.z, ry * s.w);
+        double rds = fma(rx, a.x, ry * a.y);
+        double inv = rcp_or_zero(rho2);
+        double c = rdn * rds * inv * inv;
+        tx[q] = fma(c, rx, tx[q]);
+        ty[q] = fma(c, ry, ty[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < FAR_TPT; ++q) {
+      bool use = true;
+      if (MASK) use = !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
+      if (use) { ax[q] += tx[q]; ay[q] += ty[q]; }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < FAR_TPT; ++q) {
+    int i = i0 + q * FAR_NT;
+    if (i < N) partial[(size_t)split * N + i] = make_double2(ax[q], ay[q]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Near field: barycentric evaluation (Barnett-Wu-Veerapaneni) of the Stokes
+// double layer of one curve as five holomorphic evaluations
+// (StokesInteriorDLP/StokesExteriorDLP, stokesSolver.f:4937-5379).
+
+// The five complex fields of one node: x.sigma, sigma_x, sigma_y,
+// sigma n_x/(n_x + i n_y), sigma n_y/(n_x + i n_y) (:4984, :4992-4997,
+// :5268-5276).
+__device__ __forceinline__ void node_fields(const GeoDev& G, const double* __restrict__ den, int g,
+                                            double2 f[5]) {
+  double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+  double2 p = G.xy[g], nn = G.nrm[g];
+  f[0] = make_double2(p.x * sx + p.y * sy, 0.0);
+  f[1] = make_double2(sx, 0.0);
+  f[2] = make_double2(sy, 0.0);
+  double2 ninv = cinv(nn);
+  f[3] = cmul(make_double2(sx * nn.x, sy * nn.x), ninv);
+  f[4] = cmul(make_double2(sx * nn.y, sy * nn.y), ninv);
+}
+
+// Boundary values of the five fields on one source curve
+// (compute_bdval_in :5103-5146, compute_bdval_ex :5382-5427):
+//   S_j = -sum_{k != j} (f_k - f_j) z'_k dt/(z_k - z_j) - dt f'_j
+//   interior: -i S_j/(2pi) - f_j        exterior: i S_j/(2pi)
+// with f' the spectral derivative.  One CTA per (curve, 256 nodes j).
+__global__ void __launch_bounds__(BD_NT)
+k_bdval(GeoDev G, const double* __restrict__ den, const int2* __restrict__ work,
+        const int* __restrict__ src_curve, const long long* __restrict__ bd_off,
+        const double* __restrict__ dker_wall, const double* __restrict__ dker_body,
+        double2* __restrict__ bd) {
+  __shared__ double2 sz[BD_NT], sdz[BD_NT];
+  __shared__ double2 sf[5][BD_NT];
+  const int s = work[blockIdx.x].x, j0 = work[blockIdx.x].y;
+  const int c = src_curve[s];
+  const int start = curve_start(G, c), len = curve_len(G, c);
+  const double* __restrict__ dk = (c == 0) ? dker_wall : dker_body;
+  const int j = j0 + threadIdx.x;
+  const bool act = j < len;
+  const int jc = act ? j : len - 1;
+  const double2 zj = G.xy[start + jc];
+  double2 fj[5];
+  node_fields(G, den, start + jc, fj);
+  double2 S[5], D[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) { S[q] = make_double2(0, 0); D[q] = make_double2(0, 0); }
+  for (int k0 = 0; k0 < len; k0 += BD_NT) {
+    __syncthreads();
+    const int kl = k0 + threadIdx.x;
+    if (kl < len) {
+      const int g = start + kl;
+      sz[threadIdx.x] = G.xy[g];
+      sdz[threadIdx.x] = G.dz[g];
+      double2 f[5];
+      node_fields(G, den, g, f);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) sf[q][threadIdx.x] = f[q];
+    }
+    __syncthreads();
+    const int kt = min(BD_NT, len - k0);
+    for (int kk = 0; kk < kt; ++kk) {
+      const int k = k0 + kk;
+      int m = jc - k;
+      if (m < 0) m += len;
+      const double dd = __ldg(dk + m);
+      double2 cc = make_double2(0.0, 0.0);
+      if (k != jc) cc = cmul(sdz[kk], cinv(csub(sz[kk], zj)));
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const double2 fk = sf[q][kk];
+        D[q].x = fma(dd, fk.x, D[q].x);
+        D[q].y = fma(dd, fk.y, D[q].y);
+        const double2 df = csub(fk, fj[q]);
+        S[q].x -= df.x * cc.x - df.y * cc.y;
+        S[q].y -= df.x * cc.y + df.y * cc.x;
+      }
+    }
+  }
+  if (!act) return;
+  const double h = EB_TWOPI / len;
+  const long long base = bd_off[s];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double2 Sq = make_double2(S[q].x - h * D[q].x, S[q].y - h * D[q].y);
+    double2 r;
+    if (c == 0) r = make_double2(Sq.y / EB_TWOPI - fj[q].x, -Sq.x / EB_TWOPI - fj[q].y);
+    else r = make_double2(-Sq.y / EB_TWOPI, Sq.x / EB_TWOPI);
+    bd[base + (long long)q * len + j] = r;
+  }
+}
+
+// Source-curve tile of the barycentric kernels.
+struct BaryTile {
+  double2 z[NEAR_TK], dz[NEAR_TK], za[NEAR_TK], b[5][NEAR_TK];
+};
+
+__device__ __forceinline__ void bary_load_tile(BaryTile& T, const GeoDev& G, int start, int len, int k0,
+                                               const double2* __restrict__ bdc, bool ext, double2 a) {
+  __syncthreads();
+  for (int t = threadIdx.x; t < NEAR_TK; t += blockDim.x) {
+    int k = k0 + t;
+    if (k < len) {
+      int g = start + k;
+      double2 z = G.xy[g];
+      T.z[t] = z;
+      T.dz[t] = G.dz[g];
+      T.za[t] = ext ? cinv(csub(z, a)) : make_double2(0, 0);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) T.b[q][t] = bdc[(long long)q * len + k];
+    }
+  }
+  __syncthreads();
+}
+
+// Result of one barycentric Stokes evaluation.
+struct DLPVal {
+  double ux, uy, u1x, u1y, u2x, u2y;
+};
+
+// The coincident-node branch of laplaceExteriorHolomorphic (:5492-5506) for
+// field q, evaluated from global memory (taken only when a target lies
+// within 1e-10 of a source node).
+__device__ double2 bary_coincident(const GeoDev& G, int start, int len, const double2* __restrict__ bdc, int q,
+                                   int k, double2 zt, double2 a, double2& tmp1, double2& tmp2) {
+  const double2 bk = bdc[(long long)q * len + k];
+  const double2 zk = G.xy[start + k];
+  for (int l = 0; l < len; ++l) {
+    const double2 zl = G.xy[start + l], dzl = G.dz[start + l];
+    const double2 bl = bdc[(long long)q * len + l];
+    const double2 zla = csub(zl, a), zlt = csub(zl, zt);
+    if (l != k) {
+      double2 t = csub(cmul(bk, cdiv(csub(zk, a), zla)), bl);
+      tmp1 = cadd(tmp1, cdiv(cmul(t, dzl), zlt));
+    }
+    tmp2 = cadd(tmp2, cmul(cinv(cmul(zla, zlt)), dzl));
+  }
+  const double2 dk = csub(zk, zt);
+  double2 t = csub(cdiv(tmp1, tmp2), cmul(dk, bk));
+  t = cdiv(t, cmul(dk, dk));
+  t = cdiv(t, csub(zt, a));
+  return cmul(t, G.dz[start + k]);
+}
+
+// Evaluates the Stokes DLP (and for NDER = 2 its gradient) of source curve c
+// at the target zt.  All threads of the CTA call it for the same curve; the
+// curve is streamed through shared memory three times (value, first and
+// second derivative passes, :5190-5228 / :5468-5525).
+template <int NDER>
+__device__ DLPVal bary_eval(BaryTile& T, const GeoDev& G, int c, const double2* __restrict__ bdc, double2 zt,
+                            bool act) {
+  const int start = curve_start(G, c), len = curve_len(G, c);
+  const bool ext = c != 0;
+  double2 a = make_double2(0, 0);
+  if (ext) a = G.cen[c - 1];
+  // Pass 1: values.
+  double2 den = make_double2(0, 0), num[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) num[q] = make_double2(0, 0);
+  for (int k0 = 0; k0 < len; k0 += NEAR_TK) {
+    bary_load_tile(T, G, start, len, k0, bdc, ext, a);
+    const int kt = min(NEAR_TK, len - k0);
+    for (int kk = 0; kk < kt; ++kk) {
+      const double2 c1 = cmul(T.dz[kk], cinv(csub(T.z[kk], zt)));
+      den = cadd(den, c1);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) cfma(num[q], T.b[q][kk], c1);
+    }
+  }
+  double2 u[5];
+  {
+    const double2 dd = ext ? make_double2(den.x, den.y - EB_TWOPI) : den;
+    const double2 di = cinv(dd);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) u[q] = cmul(num[q], di);
+  }
+  // Pass 2: first derivative.
+  double2 den2 = make_double2(0, 0), num2[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) num2[q] = make_double2(0, 0);
+  bool coinc = false;
+  for (int k0 = 0; k0 < len; k0 += NEAR_TK) {
+    bary_load_tile(T, G, start, len, k0, bdc, ext, a);
+    const int kt = min(NEAR_TK, len - k0);
+    for (int kk = 0; kk < kt; ++kk) {
+      const double2 d = csub(T.z[kk], zt);
+      const double2 inv = cinv(d);
+      const double2 c1 = cmul(T.dz[kk], inv);
+      if (ext) {
+        den2 = cadd(den2, cmul(c1, T.za[kk]));
+        if (cabs2(d) <= 1e-20) { coinc = true; continue; }
+      }
+      const double2 c2 = cmul(c1, inv);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) cfma(num2[q], csub(T.b[q][kk], u[q]), c2);
+    }
+  }
+  if (ext && coinc && act) {
+#pragma unroll 1
+    for (int q = 0; q < 5; ++q) {
+      double2 tmp1 = make_double2(0, 0), tmp2 = make_double2(0, 0);
+      for (int k = 0; k < len; ++k) {
+        const double2 d = csub(G.xy[start + k], zt);
+        if (cabs2(d) <= 1e-20) num2[q] = cadd(num2[q], bary_coincident(G, start, len, bdc, q, k, zt, a, tmp1, tmp2));
+      }
+    }
+  }
+  double2 du[5];
+  double2 fac;
+  if (ext) fac = cinv(cmul(csub(zt, a), den2));
+  else fac = cinv(den);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) du[q] = cmul(num2[q], fac);
+  DLPVal r;
+  r.ux = du[0].x - zt.x * du[1].x - zt.y * du[2].x + u[3].x;
+  r.uy = -du[0].y + zt.x * du[1].y + zt.y * du[2].y + u[4].x;
+  r.u1x = r.u1y = r.u2x = r.u2y = 0.0;
+  if (NDER == 2) {
+    // Pass 3: second derivative.
+    double2 num3[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) num3[q] = make_double2(0, 0);
+    for (int k0 = 0; k0 < len; k0 += NEAR_TK) {
+      bary_load_tile(T, G, start, len, k0, bdc, ext, a);
+      const int kt = min(NEAR_TK, len - k0);
+      for (int kk = 0; kk < kt; ++kk) {
+        const double2 d = csub(T.z[kk], zt);
+        const double2 inv = cinv(d);
+        const double2 c3 = cmul(cmul(cmul(T.dz[kk], inv), inv), inv);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double2 t = csub(csub(T.b[q][kk], u[q]), cmul(du[q], d));
+          cfma(num3[q], t, c3);
+        }
+      }
+    }
+    double2 dd[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) dd[q] = cscale(cmul(num3[q], fac), 2.0);
+    r.u1x = dd[0].x - du[1].x - zt.x * dd[1].x - zt.y * dd[2].x + du[3].x;
+    r.u1y = -dd[0].y + zt.x * dd[1].y - du[2].x + zt.y * dd[2].y - du[3].y;
+    r.u2x = -dd[0].y + du[1].y + zt.x * dd[1].y + zt.y * dd[2].y + du[4].x;
+    r.u2y = -dd[0].x + zt.x * dd[1].x + du[2].y + zt.y * dd[2].x - du[4].y;
+  }
+  return r;
+}
+
+// Near-pair list evaluation: CTA = (source s, pairs [p0, p1)), one thread per
+// (target, source curve) pair.  Output: (ux, uy) per pair.
+__global__ void __launch_bounds__(NEAR_NT)
+k_bary_list(GeoDev G, const int4* __restrict__ work, const int* __restrict__ src_curve,
+            const long long* __restrict__ bd_off, const double2* __restrict__ bd,
+            const int* __restrict__ pair_tgt, const double2* __restrict__ txy, double2* __restrict__ out) {
+  __shared__ BaryTile T;
+  const int4 wk = work[blockIdx.x];
+  const int s = wk.x, p0 = wk.y, p1 = wk.z;
+  const int c = src_curve[s];
+  const int p = p0 + threadIdx.x;
+  const bool act = p < p1;
+  const double2 zt = txy[pair_tgt[act ? p : p1 - 1]];
+  DLPVal r = bary_eval<1>(T, G, c, bd + bd_off[s], zt, act);
+  if (act) out[p] = make_double2(r.ux, r.uy);
+}
+
+// ---------------------------------------------------------------------------
+// Assembles the boundary operator for every node: far-field partial sums,
+// barycentric pairs (in a fixed order per target), the diagonal curvature
+// limit and jump (:937-951, :964-985), stokeslets and rotlets of every body
+// (:992-1049) and the wall's rank-one term (:1115-1118).
+constexpr int SR_CHUNK = 256;
+__global__ void __launch_bounds__(256)
+k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ partial, int nsplit,
+          const int* __restrict__ tptr, const int* __restrict__ tpairs, const double2* __restrict__ pair_out,
+          const double* __restrict__ sigdotn, double* __restrict__ vel) {
+  __shared__ double4 sc[SR_CHUNK];   // cx, cy, stokeslet x, stokeslet y
+  __shared__ double sr[SR_CHUNK];    // rotlet
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = g < G.N;
+  const int gc = act ? g : G.N - 1;
+  const double2 p = G.xy[gc];
+  double ux = 0.0, uy = 0.0;
+  for (int q = 0; q < nsplit; ++q) {
+    double2 v = partial[(size_t)q * G.N + gc];
+    ux += v.x; uy += v.y;
+  }
+  if (tptr) {
+    for (int e = tptr[gc]; e < tptr[gc + 1]; ++e) {
+      double2 v = pair_out[tpairs[e]];
+      ux += v.x; uy += v.y;
+    }
+  }
+  const long long ixg = ix_of(G, gc), iyg = iy_of(G, gc);
+  const double sx = den[ixg], sy = den[iyg];
+  const double2 nn = G.nrm[gc];
+  const double cu = G.cur[gc], s = G.sp[gc];
+  const int nc = gc < G.nout ? G.nout : G.n;
+  const double tdd = nn.y * sx - nn.x * sy;
+  ux = ux - cu * tdd * nn.y * s / nc;
+  uy = uy + cu * tdd * nn.x * s / nc;
+  ux -= 0.5 * sx;
+  uy -= 0.5 * sy;
+  for (int b0 = 0; b0 < G.M; b0 += SR_CHUNK) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < SR_CHUNK; t += blockDim.x) {
+      int b = b0 + t;
+      if (b < G.M) {
+        double2 cc = G.cen[b];
+        sc[t] = make_double4(cc.x, cc.y, den[ic_of(G, b, 0)], den[ic_of(G, b, 1)]);
+        sr[t] = den[ic_of(G, b, 2)];
+      }
+    }
+    __syncthreads();
+    const int bt = min(SR_CHUNK, G.M - b0);
+    for (int t = 0; t < bt; ++t) {
+      const double4 q = sc[t];
+      const double rot = sr[t];
+      const double rx = p.x - q.x, ry = p.y - q.y;
+      const double rho2 = rx * rx + ry * ry;
+      const double rd = rx * q.z + ry * q.w;
+      const double lg = log(rho2);
+      const double ir = 1.0 / rho2;
+      ux += 0.5 / EB_TWOPI * (-0.5 * lg * q.z + rd * ir * rx) + rot * ry * ir;
+      uy += 0.5 / EB_TWOPI * (-0.5 * lg * q.w + rd * ir * ry) - rot * rx * ir;
+    }
+  }
+  if (gc < G.nout) {
+    const double sg = *sigdotn;
+    ux += sg * nn.x;
+    uy += sg * nn.y;
+  }
+  if (act) { vel[ixg] = ux; vel[iyg] = uy; }
+}
+
+// Right-hand side of bd_condition (:208-314).
+__global__ void k_rhs(GeoDev G, int ibc, int mode, double wall_b, double* __restrict__ rhs) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < G.M * 3) rhs[2LL * G.nout + 2LL * G.n * G.M + g] = 0.0;
+  if (g >= G.N) return;
+  const double2 p = G.xy[g];
+  double u = 0.0, v = 0.0;
+  if (mode == 2) {
+    u = 0.0;   // homogeneous data (used to exercise the zero right-hand-side path)
+  } else if (mode == 1) {
+    const double s1 = 1.0, s2 = 2.0, rot = 3.0;
+    double rx = p.x, ry = p.y, rd = rx * s1 + ry * s2, rho2 = rx * rx + ry * ry;
+    u = 0.5 / EB_TWOPI * (-0.5 * log(rho2) * s1 + rd / rho2 * rx) + rot * ry / rho2;
+    v = 0.5 / EB_TWOPI * (-0.5 * log(rho2) * s2 + rd / rho2 * ry) - rot * rx / rho2;
+  } else if (g < G.nout) {
+    if (ibc == 0) u = (1.0 + p.y / wall_b) * (1.0 - p.y / wall_b);
+    else u = 1.0;
+  }
+  rhs[ix_of(G, g)] = u;
+  rhs[iy_of(G, g)] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Krylov kernels (tall-skinny products with the basis V, row-major by vector).
+
+// part[j*gridDim.x + blk] = sum over this CTA's rows of V[j] . w
+__global__ void __launch_bounds__(256)
+k_dot_part(const double* __restrict__ V, long long ldv, int k, const double* __restrict__ w, long long n,
+           int R, double* __restrict__ part) {
+  extern __shared__ double swv[];
+  const long long r0 = (long long)blockIdx.x * R;
+  const int rl = (int)max(0LL, min((long long)R, n - r0));
+  for (int t = threadIdx.x; t < rl; t += blockDim.x) swv[t] = w[r0 + t];
+  __syncthreads();
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = wid; j < k; j += nw) {
+    const double* __restrict__ vj = V + (long long)j * ldv + r0;
+    double s = 0.0;
+    for (int t = lane; t < rl; t += 32) s = fma(__ldg(vj + t), swv[t], s);
+    s = warp_sum(s);
+    if (lane == 0) part[(size_t)j * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// h[j] (+)= sum_b part[j][b]; one warp per j.
+__global__ void k_dot_reduce(const double* __restrict__ part, int nb, int k, double* __restrict__ h, int accumulate) {
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= k) return;
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += part[(size_t)j * nb + b];
+  s = warp_sum(s);
+  if (lane == 0) h[j] = accumulate ? h[j] + s : s;
+}
+
+// w[i] += sign * sum_j V[j][i] h[j]
+__global__ void __launch_bounds__(256)
+k_vh(const double* __restrict__ V, long long ldv, int k, const double* __restrict__ h, double sign,
+     double* __restrict__ w, long long n) {
+  __shared__ double sh[1024];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  for (int j0 = 0; j0 < k; j0 += 1024) {
+    const int jt = min(1024, k - j0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < jt; t += blockDim.x) sh[t] = h[j0 + t];
+    __syncthreads();
+    if (i < n) {
+      const double* __restrict__ vp = V + (long long)j0 * ldv + i;
+      int j = 0;
+      double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+      for (; j + 3 < jt; j += 4) {
+        a0 = fma(__ldg(vp + (long long)(j)*ldv), sh[j], a0);
+        a1 = fma(__ldg(vp + (long long)(j + 1) * ldv), sh[j + 1], a1);
+        a2 = fma(__ldg(vp + (long long)(j + 2) * ldv), sh[j + 2], a2);
+        a3 = fma(__ldg(vp + (long long)(j + 3) * ldv), sh[j + 3], a3);
+      }
+      for (; j < jt; ++j) a0 = fma(__ldg(vp + (long long)j * ldv), sh[j], a0);
+      acc += (a0 + a1) + (a2 + a3);
+    }
+  }
+  if (i < n) w[i] += sign * acc;
+}
+
+__global__ void k_scale(double* __restrict__ v, double a, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] *= a;
+}
+
+// r = b - r
+__global__ void k_bminus(const double* __restrict__ b, double* __restrict__ r, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = b[i] - r[i];
+}
+
+// out = a (copy) — used to seed the basis from a residual.
+__global__ void k_copy(const double* __restrict__ a, double* __restrict__ out, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i];
+}
+
+}  // namespace

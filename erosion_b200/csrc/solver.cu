@@ -1,0 +1,710 @@
+// Host orchestration of the boundary operator and the GMRES solve, and the
+// C ABI entry points that replace the reference's libstokes.so.
+#include "state.h"
+#include "kernels.cuh"
+#include <cmath>
+#include <cstring>
+
+namespace eb {
+
+State& state() {
+  static State s;
+  return s;
+}
+
+static int g_num_sms = 148;
+int eb_num_sms() { return g_num_sms; }
+
+void ensure_init(State& s) {
+  if (s.init) return;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    throw Error(EROSION_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  EB_CK(cudaGetDevice(&s.device));
+  cudaDeviceProp prop;
+  EB_CK(cudaGetDeviceProperties(&prop, s.device));
+  g_num_sms = prop.multiProcessorCount;
+  EB_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+  EB_CK(cudaEventCreate(&s.e0));
+  EB_CK(cudaEventCreate(&s.e1));
+  EB_CK(cudaEventCreate(&s.ef0));
+  EB_CK(cudaEventCreate(&s.ef1));
+  s.init = true;
+}
+
+// The circulant matrix of fourierDiff (stokesSolver.f:348-388) for even n:
+// d[m] = (1/2)(-1)^m cot(pi m/n), d[0] = d[n/2] = 0.
+static std::vector<double> spectral_kernel(int n) {
+  std::vector<double> d(n, 0.0);
+  const double pi = 4.0 * std::atan(1.0);
+  for (int m = 1; m < n; ++m) {
+    if (2 * m == n) continue;
+    double t = pi * m / n;
+    d[m] = 0.5 * ((m & 1) ? -1.0 : 1.0) * std::cos(t) / std::sin(t);
+  }
+  return d;
+}
+
+static void build_near(State& s, const std::vector<double2>& hxy, const std::vector<double>& hsp,
+                       const std::vector<double2>& hcen, const std::vector<double>& hrb) {
+  const Problem& pr = s.pr;
+  const int n = pr.n, M = pr.M, nout = pr.nout, N = pr.N;
+  const double TWOPI = 8.0 * std::atan(1.0);
+  Near& nr = s.near;
+  // matvec_DLP_fmmbary's wall length scale: 'lw' is an implicitly typed
+  // INTEGER there (stokesSolver.f:705-709), so each partial sum truncates and
+  // the mean is an integer division.
+  long long lw = 0;
+  for (int k = 0; k < nout; ++k) lw = (long long)((double)lw + hsp[k]);
+  lw = lw / nout;
+  nr.lw = lw;
+  nr.wall_bodies.clear();
+
+  std::vector<int> pc, pt;   // (source curve, target node) in the reference's order
+  if (pr.P.ibary == 1 && pr.P.ifmm != 0) {
+    const double alpha1 = 4.0, alpha2 = 4.0, bw = pr.P.wall_b;
+    for (int b = 0; b < M; ++b) {   // :711-816
+      double dsum = hrb[b] + alpha2 * (double)lw * TWOPI / nout;
+      double dsum2 = bw - dsum;
+      if (std::fabs(hcen[b].y) >= dsum2) {
+        nr.wall_bodies.push_back(b);
+        for (int k = 0; k < n; ++k) {
+          int g = nout + b * n + k;
+          if (std::fabs(hxy[g].y) >= dsum2) { pc.push_back(0); pt.push_back(g); }
+        }
+        double r = bw - std::fabs(hcen[b].y) + 2.0 * hrb[b];
+        for (int j = 0; j < nout; ++j) {
+          double dx = hcen[b].x - hxy[j].x, dy = hcen[b].y - hxy[j].y;
+          if (dx * dx + dy * dy <= r * r) { pc.push_back(1 + b); pt.push_back(j); }
+        }
+      }
+    }
+    for (int sb = 0; sb < M; ++sb) {   // :838-926
+      for (int t = 0; t < M; ++t) {
+        if (t == sb) continue;
+        double dx = hcen[sb].x - hcen[t].x, dy = hcen[sb].y - hcen[t].y;
+        double d2 = dx * dx + dy * dy;
+        double rsum = hrb[sb] + hrb[t] + alpha1 * (hrb[sb] + hrb[t]) * TWOPI / n;
+        if (d2 <= rsum * rsum) {
+          for (int k = 0; k < n; ++k) {
+            int g = nout + t * n + k;
+            double ex = hcen[sb].x - hxy[g].x, ey = hcen[sb].y - hxy[g].y;
+            if (ex * ex + ey * ey <= rsum * rsum) { pc.push_back(1 + sb); pt.push_back(g); }
+          }
+        }
+      }
+    }
+  } else if (pr.P.ibary == 1) {
+    // matvec_DLP_bary (:1128-1516): every pair of distinct curves.
+    for (int g = nout; g < N; ++g) { pc.push_back(0); pt.push_back(g); }
+    for (int sb = 0; sb < M; ++sb) {
+      for (int g = 0; g < N; ++g) {
+        if (g >= nout && (g - nout) / n == sb) continue;
+        pc.push_back(1 + sb); pt.push_back(g);
+      }
+    }
+  }
+  const long long P = (long long)pc.size();
+  nr.npairs = P;
+  nr.mw = (M + 1 + 31) / 32;
+  if (P == 0) { nr.nsrc = 0; nr.n_bd_work = nr.n_bary_work = 0; return; }
+  // group by source curve, stable
+  std::vector<long long> cnt(M + 2, 0);
+  for (long long p = 0; p < P; ++p) cnt[pc[p] + 1]++;
+  for (int c = 0; c <= M; ++c) cnt[c + 1] += cnt[c];
+  std::vector<int> order(P);
+  {
+    std::vector<long long> pos(cnt.begin(), cnt.end() - 1);
+    for (long long p = 0; p < P; ++p) order[pos[pc[p]]++] = (int)p;
+  }
+  nr.h_src_curve.clear(); nr.h_src_ptr.clear(); nr.h_pair_tgt.assign(P, 0);
+  std::vector<long long> hbdoff;
+  std::vector<int2> hbdw;
+  std::vector<int4> hbw;
+  long long bdtot = 0;
+  for (int c = 0; c <= M; ++c) {
+    if (cnt[c + 1] == cnt[c]) continue;
+    int sidx = (int)nr.h_src_curve.size();
+    nr.h_src_curve.push_back(c);
+    nr.h_src_ptr.push_back((int)cnt[c]);
+    int len = c == 0 ? nout : n;
+    hbdoff.push_back(bdtot);
+    bdtot += 5LL * len;
+    for (int j0 = 0; j0 < len; j0 += BD_NT) hbdw.push_back(make_int2(sidx, j0));
+    for (long long p0 = cnt[c]; p0 < cnt[c + 1]; p0 += NEAR_NT)
+      hbw.push_back(make_int4(sidx, (int)p0, (int)std::min<long long>(p0 + NEAR_NT, cnt[c + 1]), 0));
+  }
+  nr.h_src_ptr.push_back((int)P);
+  for (long long q = 0; q < P; ++q) nr.h_pair_tgt[q] = pt[order[q]];
+  nr.nsrc = (int)nr.h_src_curve.size();
+  nr.bd_total = bdtot;
+  nr.n_bd_work = (int)hbdw.size();
+  nr.n_bary_work = (int)hbw.size();
+  // per-target list of pair slots (pairs are now in grouped order)
+  std::vector<int> tptr(N + 1, 0), tpairs(P);
+  for (long long q = 0; q < P; ++q) tptr[nr.h_pair_tgt[q] + 1]++;
+  for (int g = 0; g < N; ++g) tptr[g + 1] += tptr[g];
+  {
+    std::vector<int> pos(tptr.begin(), tptr.end() - 1);
+    for (long long q = 0; q < P; ++q) tpairs[pos[nr.h_pair_tgt[q]]++] = (int)q;
+  }
+  std::vector<unsigned> mask((size_t)N * nr.mw, 0u);
+  for (long long q = 0; q < P; ++q) {
+    int g = nr.h_pair_tgt[q];
+    int c = pc[order[q]];
+    mask[(size_t)g * nr.mw + (c >> 5)] |= 1u << (c & 31);
+  }
+  cudaStream_t st = s.st;
+  h2d(nr.src_curve.ensure(nr.nsrc), nr.h_src_curve.data(), nr.nsrc, st);
+  h2d(nr.pair_tgt.ensure(P), nr.h_pair_tgt.data(), P, st);
+  h2d(nr.tptr.ensure(N + 1), tptr.data(), N + 1, st);
+  h2d(nr.tpairs.ensure(P), tpairs.data(), P, st);
+  h2d(nr.bd_off.ensure(nr.nsrc), hbdoff.data(), nr.nsrc, st);
+  h2d(nr.bd_work.ensure(hbdw.size()), hbdw.data(), hbdw.size(), st);
+  h2d(nr.bary_work.ensure(hbw.size()), hbw.data(), hbw.size(), st);
+  h2d(nr.mask.ensure(mask.size()), mask.data(), mask.size(), st);
+  s.bd.ensure(bdtot);
+  s.pair_out.ensure(P);
+  EB_CK(cudaStreamSynchronize(st));   // host vectors go out of scope
+}
+
+static void build_tiles(State& s) {
+  const Problem& pr = s.pr;
+  std::vector<int4> tl;
+  auto add = [&](int start, int len, int c) {
+    for (int o = 0; o < len; o += FAR_TS) tl.push_back(make_int4(start + o, std::min(FAR_TS, len - o), c, 0));
+  };
+  add(0, pr.nout, 0);
+  for (int b = 0; b < pr.M; ++b) add(pr.nout + b * pr.n, pr.n, 1 + b);
+  s.ntile = (int)tl.size();
+  int TB = (int)nblk(pr.N, FAR_NT * FAR_TPT);
+  int want = (int)std::ceil(8.0 * g_num_sms / TB);
+  s.nsplit = std::max(1, std::min(want, s.ntile));
+  std::vector<int> sp(s.nsplit + 1);
+  for (int q = 0; q <= s.nsplit; ++q) sp[q] = (int)((long long)q * s.ntile / s.nsplit);
+  h2d(s.tiles.ensure(tl.size()), tl.data(), tl.size(), s.st);
+  h2d(s.split_ptr.ensure(sp.size()), sp.data(), sp.size(), s.st);
+  s.partial.ensure((size_t)s.nsplit * pr.N);
+  EB_CK(cudaStreamSynchronize(s.st));
+}
+
+void setup_problem(State& s, const Problem& in, const double* d_xx, const double* d_yy) {
+  Problem pr = in;
+  if (pr.nout < 8 || (pr.nout & 1)) throw Error(EROSION_BAD_INPUT, "nouter must be even and >= 8");
+  if (pr.M < 0) throw Error(EROSION_BAD_INPUT, "nbods must be >= 0");
+  if (pr.M > 0 && (pr.n < 4 || (pr.n & 1))) throw Error(EROSION_BAD_INPUT, "npts must be even and >= 4");
+  if (pr.M == 0) pr.n = std::max(pr.n, 2);
+  if (!(pr.P.wall_a > 0 && pr.P.wall_b > 0 && pr.P.wall_order > 0))
+    throw Error(EROSION_BAD_INPUT, "wall semi-axes and order must be positive");
+  if ((long long)pr.nout + (long long)pr.n * pr.M > (1LL << 30)) throw Error(EROSION_BAD_INPUT, "too many nodes");
+  pr.N = pr.nout + pr.n * pr.M;
+  pr.ntot = 2LL * pr.N + 3LL * pr.M;
+  s.pr = pr;
+  s.geo_valid = false;
+  cudaStream_t st = s.st;
+  if (s.dker_wall_n != pr.nout) {
+    auto d = spectral_kernel(pr.nout);
+    h2d(s.dker_wall.ensure(pr.nout), d.data(), pr.nout, st);
+    EB_CK(cudaStreamSynchronize(st));
+    s.dker_wall_n = pr.nout;
+  }
+  if (pr.M > 0 && s.dker_body_n != pr.n) {
+    auto d = spectral_kernel(pr.n);
+    h2d(s.dker_body.ensure(pr.n), d.data(), pr.n, st);
+    EB_CK(cudaStreamSynchronize(st));
+    s.dker_body_n = pr.n;
+  }
+  const int N = pr.N;
+  s.wx.ensure(pr.nout); s.wy.ensure(pr.nout);
+  s.xy.ensure(N); s.nrm.ensure(N); s.dz.ensure(N); s.d1tmp.ensure(N);
+  s.sp.ensure(N); s.cur.ensure(N); s.w.ensure(N);
+  s.cen.ensure(std::max(pr.M, 1)); s.rb.ensure(std::max(pr.M, 1));
+  s.ws.ensure(N); s.sigdotn.ensure(1);
+  k_wall_nodes<<<nblk(pr.nout, 256), 256, 0, st>>>(pr.nout, pr.P.wall_a, pr.P.wall_b, pr.P.wall_order, s.wx.p, s.wy.p);
+  EB_LAUNCH_CHECK();
+  k_geom<<<1, 1024, 0, st>>>(s.wx.p, s.wy.p, pr.nout, s.dker_wall.p, 0, 1, s.xy.p, s.nrm.p, s.sp.p, s.cur.p, s.w.p,
+                             s.dz.p, s.d1tmp.p);
+  EB_LAUNCH_CHECK();
+  if (pr.M > 0) {
+    k_geom<<<pr.M, 256, 0, st>>>(d_xx, d_yy, pr.n, s.dker_body.p, pr.nout, 0, s.xy.p, s.nrm.p, s.sp.p, s.cur.p,
+                                 s.w.p, s.dz.p, s.d1tmp.p + pr.nout);
+    EB_LAUNCH_CHECK();
+    k_body_stats<<<pr.M, 256, 0, st>>>(pr.n, pr.nout, s.xy.p, s.sp.p, s.cen.p, s.rb.p);
+    EB_LAUNCH_CHECK();
+  }
+  std::vector<double2> hxy(N), hcen(pr.M);
+  std::vector<double> hsp(pr.nout), hrb(pr.M);
+  d2h(hxy.data(), s.xy.p, N, st);
+  d2h(hsp.data(), s.sp.p, pr.nout, st);
+  d2h(hcen.data(), s.cen.p, pr.M, st);
+  d2h(hrb.data(), s.rb.p, pr.M, st);
+  EB_CK(cudaStreamSynchronize(st));
+  for (int g = 0; g < N; ++g)
+    if (!std::isfinite(hxy[g].x) || !std::isfinite(hxy[g].y)) throw Error(EROSION_BAD_INPUT, "non-finite node coordinates");
+  for (int k = 0; k < pr.nout; ++k)
+    if (!(hsp[k] > 0) || !std::isfinite(hsp[k])) throw Error(EROSION_BAD_INPUT, "degenerate wall geometry");
+  // Every body node must lie strictly inside the superellipse wall.
+  for (int g = pr.nout; g < N; ++g) {
+    double fx = std::pow(std::fabs(hxy[g].x) / pr.P.wall_a, pr.P.wall_order);
+    double fy = std::pow(std::fabs(hxy[g].y) / pr.P.wall_b, pr.P.wall_order);
+    if (!(fx + fy < 1.0)) throw Error(EROSION_BAD_INPUT, "a body node lies on or outside the wall");
+  }
+  build_near(s, hxy, hsp, hcen, hrb);
+  build_tiles(s);
+  s.geo_valid = true;
+}
+
+void apply_operator(State& s, const double* d_den, double* d_vel) {
+  const Problem& pr = s.pr;
+  const GeoDev G = s.geo();
+  const Near& nr = s.near;
+  cudaStream_t st = s.st;
+  k_prep<<<pr.M + 1, 256, 0, st>>>(G, d_den, s.ws.p, d_vel, s.sigdotn.p);
+  EB_LAUNCH_CHECK();
+  dim3 fg(nblk(pr.N, FAR_NT * FAR_TPT), s.nsplit);
+  EB_CK(cudaEventRecord(s.ef0, st));
+  if (nr.npairs > 0)
+    k_far64<true><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nr.mask.p, nr.mw, s.partial.p);
+  else
+    k_far64<false><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nullptr, 0, s.partial.p);
+  EB_LAUNCH_CHECK();
+  EB_CK(cudaEventRecord(s.ef1, st));
+  if (nr.npairs > 0) {
+    k_bdval<<<nr.n_bd_work, BD_NT, 0, st>>>(G, d_den, nr.bd_work.p, nr.src_curve.p, nr.bd_off.p, s.dker_wall.p,
+                                            s.dker_body.p, s.bd.p);
+    EB_LAUNCH_CHECK();
+    k_bary_list<<<nr.n_bary_work, NEAR_NT, 0, st>>>(G, nr.bary_work.p, nr.src_curve.p, nr.bd_off.p, s.bd.p,
+                                                    nr.pair_tgt.p, s.xy.p, s.pair_out.p);
+    EB_LAUNCH_CHECK();
+  }
+  k_combine<<<nblk(pr.N, 256), 256, 0, st>>>(G, d_den, s.partial.p, s.nsplit, nr.npairs ? nr.tptr.p : nullptr,
+                                             nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p, d_vel);
+  EB_LAUNCH_CHECK();
+  s.stats.matvecs++;
+  s.stats.far_launches++;
+}
+
+void build_rhs(State& s, double* d_rhs) {
+  const GeoDev G = s.geo();
+  k_rhs<<<nblk(std::max(s.pr.N, 3 * s.pr.M), 256), 256, 0, s.st>>>(G, s.pr.P.ibc, s.pr.P.rhs_mode, s.pr.P.wall_b, d_rhs);
+  EB_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Krylov helpers.
+static int dot_blocks(long long n, int* R) {
+  int nb = (int)std::min<long long>((long long)g_num_sms * 8, nblk(n, 256));
+  nb = std::max(nb, 1);
+  *R = (int)((n + nb - 1) / nb);
+  nb = (int)((n + *R - 1) / *R);
+  return nb;
+}
+
+// h[0..k) (+)= V[0..k) . w
+static void dots(State& s, const double* V, long long ldv, int k, const double* w, long long n, double* h,
+                 int accumulate) {
+  int R;
+  int nb = dot_blocks(n, &R);
+  double* part = s.part.ensure((size_t)k * nb);
+  k_dot_part<<<nb, 256, R * sizeof(double), s.st>>>(V, ldv, k, w, n, R, part);
+  EB_LAUNCH_CHECK();
+  k_dot_reduce<<<nblk(k, 8), 256, 0, s.st>>>(part, nb, k, h, accumulate);
+  EB_LAUNCH_CHECK();
+}
+
+double device_norm(State& s, const double* d_v, long long n) {
+  double* h = s.hdev.ensure(8);
+  dots(s, d_v, n, 1, d_v, n, h, 0);
+  double r = 0;
+  d2h(&r, h, 1, s.st);
+  EB_CK(cudaStreamSynchronize(s.st));
+  return std::sqrt(r);
+}
+
+static double* pinned(State& s, size_t n) {
+  if (n > s.h_pinned_cap) {
+    if (s.h_pinned) cudaFreeHost(s.h_pinned);
+    s.h_pinned = nullptr;
+    size_t m = std::max<size_t>(n, 4096);
+    EB_CK(cudaMallocHost((void**)&s.h_pinned, m * sizeof(double)));
+    s.h_pinned_cap = m;
+  }
+  return s.h_pinned;
+}
+
+int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl_in, double tol,
+                long long* iters, double* est) {
+  const long long N = s.pr.ntot;
+  const long long ldv = (N + 31) & ~31LL;
+  long long MAXL = maxl_in;
+  if (MAXL == 0) MAXL = 10;
+  if (MAXL > N) MAXL = N;
+  *iters = 0;
+  cudaStream_t st = s.st;
+  const double bnrm = device_norm(s, d_b, N);
+  double* r = s.d_r.ensure(N);
+  if (x0_zero) {
+    k_copy<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
+    EB_LAUNCH_CHECK();
+  } else {
+    apply_operator(s, d_x, r);
+    k_bminus<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
+    EB_LAUNCH_CHECK();
+  }
+  long long cap0 = std::min<long long>(MAXL + 1, 64);
+  if (s.vcap < cap0 || (long long)s.V.cap < cap0 * ldv) {
+    s.V.ensure((size_t)cap0 * ldv);
+    s.vcap = cap0;
+  } else {
+    s.vcap = (long long)(s.V.cap / ldv);
+  }
+  k_copy<<<nblk(N, 256), 256, 0, st>>>(r, s.V.p, N);
+  EB_LAUNCH_CHECK();
+  const double r0nrm = device_norm(s, s.V.p, N);
+  if (bnrm == 0.0) {
+    EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
+    EB_CK(cudaStreamSynchronize(st));
+    *est = 0.0;
+    throw Error(EROSION_BAD_INPUT, "zero right-hand side: the zero density was returned");
+  }
+  *est = r0nrm / bnrm;
+  if (!std::isfinite(r0nrm)) throw Error(EROSION_BREAKDOWN, "non-finite initial residual");
+  if (*est <= tol) return EROSION_OK;
+  k_scale<<<nblk(N, 256), 256, 0, st>>>(s.V.p, 1.0 / r0nrm, N);
+  EB_LAUNCH_CHECK();
+
+  std::vector<std::vector<double>> HES;   // column ll-1 holds HES(1..ll+1, ll)
+  std::vector<double> Q;
+  double prod = 1.0, rho = r0nrm;
+  long long lgmr = 0;
+  int iflag = -1;
+  double* hdev = s.hdev.ensure((size_t)MAXL + 2);
+  double* hp = pinned(s, (size_t)MAXL + 2);
+  for (long long ll = 1; ll <= MAXL; ++ll) {
+    lgmr = ll;
+    if (ll + 1 > s.vcap) {
+      long long nc = std::min<long long>(MAXL + 1, std::max<long long>(2 * s.vcap, ll + 1));
+      s.V.grow_keep((size_t)nc * ldv, (size_t)ll * ldv, st);
+      s.vcap = nc;
+    }
+    double* V = s.V.p;
+    double* vnew = V + ll * ldv;
+    apply_operator(s, V + (ll - 1) * ldv, vnew);
+    // Classical Gram-Schmidt, applied twice.
+    const int k = (int)ll;
+    dots(s, V, ldv, k, vnew, N, hdev, 0);
+    k_vh<<<nblk(N, 256), 256, 0, st>>>(V, ldv, k, hdev, -1.0, vnew, N);
+    EB_LAUNCH_CHECK();
+    double* hs = s.ydev.ensure((size_t)MAXL + 2);   // second-pass coefficients
+    dots(s, V, ldv, k, vnew, N, hs, 0);
+    k_vh<<<nblk(N, 256), 256, 0, st>>>(V, ldv, k, hs, -1.0, vnew, N);
+    EB_LAUNCH_CHECK();
+    dots(s, vnew, N, 1, vnew, N, hdev + k, 0);
+    d2h(hp, hdev, (size_t)k + 1, st);
+    std::vector<double> h2h(k);
+    d2h(h2h.data(), hs, (size_t)k, st);
+    EB_CK(cudaStreamSynchronize(st));
+    const double snormw = std::sqrt(hp[k]);
+    std::vector<double> col(ll + 1);
+    for (int i = 0; i < k; ++i) col[i] = hp[i] + h2h[i];
+    col[ll] = snormw;
+    bool finite = std::isfinite(snormw);
+    for (int i = 0; i < k && finite; ++i) finite = std::isfinite(col[i]);
+    if (!finite) { iflag = 3; break; }
+    // DHEQR (gmres_routines.f:1148), update of the last column.
+    for (long long kk = 1; kk <= ll - 1; ++kk) {
+      double c = Q[2 * (kk - 1)], sn = Q[2 * (kk - 1) + 1];
+      double t1 = col[kk - 1], t2 = col[kk];
+      col[kk - 1] = c * t1 - sn * t2;
+      col[kk] = sn * t1 + c * t2;
+    }
+    double t1 = col[ll - 1], t2 = col[ll], c, sn;
+    if (t2 == 0.0) { c = 1; sn = 0; }
+    else if (std::fabs(t2) >= std::fabs(t1)) { double t = t1 / t2; sn = -1.0 / std::sqrt(1.0 + t * t); c = -sn * t; }
+    else { double t = t2 / t1; c = 1.0 / std::sqrt(1.0 + t * t); sn = -c * t; }
+    Q.push_back(c); Q.push_back(sn);
+    col[ll - 1] = c * t1 - sn * t2;
+    HES.push_back(col);
+    if (col[ll - 1] == 0.0) { iflag = 2; break; }
+    prod = prod * sn;
+    rho = std::fabs(prod * r0nrm);
+    *est = rho / bnrm;
+    if (*est <= tol) { iflag = 0; break; }
+    if (ll == MAXL) { iflag = (rho < r0nrm) ? 1 : 2; break; }
+    k_scale<<<nblk(N, 256), 256, 0, st>>>(vnew, 1.0 / snormw, N);
+    EB_LAUNCH_CHECK();
+  }
+  *iters = lgmr;
+  if (iflag == 3) throw Error(EROSION_BREAKDOWN, "non-finite value in the Arnoldi process");
+  if (iflag == 2) return EROSION_BREAKDOWN;
+  // DHELS (gmres_routines.f:1048) and x += V y.
+  const long long L = lgmr;
+  std::vector<double> y(L + 1, 0.0);
+  y[0] = r0nrm;
+  for (long long kk = 1; kk <= L; ++kk) {
+    double c = Q[2 * (kk - 1)], sn = Q[2 * (kk - 1) + 1];
+    double a1 = y[kk - 1], a2 = y[kk];
+    y[kk - 1] = c * a1 - sn * a2;
+    y[kk] = sn * a1 + c * a2;
+  }
+  for (long long kb = 1; kb <= L; ++kb) {
+    long long kk = L + 1 - kb;
+    y[kk - 1] = y[kk - 1] / HES[kk - 1][kk - 1];
+    double t = -y[kk - 1];
+    for (long long i = 1; i <= kk - 1; ++i) y[i - 1] += t * HES[kk - 1][i - 1];
+  }
+  double* yd = s.ydev.ensure((size_t)L + 1);
+  h2d(yd, y.data(), (size_t)L, st);
+  k_vh<<<nblk(N, 256), 256, 0, st>>>(s.V.p, ldv, (int)L, yd, 1.0, d_x, N);
+  EB_LAUNCH_CHECK();
+  EB_CK(cudaStreamSynchronize(st));
+  return iflag == 1 ? EROSION_MAXITER : EROSION_OK;
+}
+
+}  // namespace eb
+
+// ===========================================================================
+// C ABI
+using namespace eb;
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  try {
+    ensure_init(s);
+    int rc = f(s);
+    s.status = rc;
+    s.err = rc == EROSION_OK ? "" : (rc == EROSION_MAXITER ? "GMRES reached maxl before the tolerance"
+                                                            : (rc == EROSION_BREAKDOWN ? "GMRES stalled" : "error"));
+    return rc;
+  } catch (const Error& e) {
+    s.status = e.code;
+    s.err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    s.status = EROSION_CUDA_ERROR;
+    s.err = e.what();
+    return EROSION_CUDA_ERROR;
+  }
+}
+
+Problem make_problem(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter) {
+  if (npts < 0 || nbods < 0 || nouter < 0 || npts > (1 << 24) || nbods > (1 << 24) || nouter > (1 << 26))
+    throw Error(EROSION_BAD_INPUT, "negative or oversized sizes");
+  Problem pr;
+  if (p) pr.P = *p;
+  else erosion_default_params(&pr.P);
+  pr.n = (int)npts; pr.M = (int)nbods; pr.nout = (int)nouter;
+  return pr;
+}
+
+// Copies body nodes to the device and sets the problem up.
+void setup_from_host(State& s, const Problem& pr, const double* xx, const double* yy) {
+  size_t nb = (size_t)pr.n * pr.M;
+  double* dx = s.d_xx.ensure(std::max<size_t>(nb, 1));
+  double* dy = s.d_yy.ensure(std::max<size_t>(nb, 1));
+  h2d(dx, xx, nb, s.st);
+  h2d(dy, yy, nb, s.st);
+  setup_problem(s, pr, dx, dy);
+}
+
+int solve_device_impl(State& s, double* d_den, bool x0_zero, int64_t* nits) {
+  const Problem& pr = s.pr;
+  s.stats = erosion_solve_stats{};
+  EB_CK(cudaEventRecord(s.e0, s.st));
+  double* rhs = s.d_rhs.ensure(pr.ntot);
+  build_rhs(s, rhs);
+  long long it = 0;
+  double est = 0;
+  int rc = gmres_solve(s, rhs, d_den, x0_zero, pr.P.maxl, pr.P.tol, &it, &est);
+  s.stats.iterations = it;
+  s.stats.sweeps = 1;
+  s.stats.est_residual = est;
+  s.stats.near_pairs = s.near.npairs;
+  if (pr.P.true_residual) {
+    double* r = s.d_w.ensure(pr.ntot);
+    apply_operator(s, d_den, r);
+    k_bminus<<<nblk(pr.ntot, 256), 256, 0, s.st>>>(rhs, r, pr.ntot);
+    EB_LAUNCH_CHECK();
+    s.stats.true_residual = device_norm(s, r, pr.ntot) / device_norm(s, rhs, pr.ntot);
+  }
+  EB_CK(cudaEventRecord(s.e1, s.st));
+  EB_CK(cudaEventSynchronize(s.e1));
+  float ms = 0;
+  EB_CK(cudaEventElapsedTime(&ms, s.e0, s.e1));
+  s.stats.ms_total = ms;
+  if (nits) *nits = it;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void erosion_default_params(erosion_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->wall_a = 3.0;
+  p->wall_b = 1.0;
+  p->wall_order = 8.0;
+  p->tol = 1e-8;
+  p->maxl = 8000;
+  p->ibary = 1;
+  p->ifmm = 1;
+  p->ibc = 1;
+  p->precision = 0;
+  p->rhs_mode = 0;
+  p->true_residual = 0;
+}
+
+int erosion_last_status(void) { return state().status; }
+const char* erosion_last_error(void) { return state().err.c_str(); }
+
+void erosion_get_solve_stats(erosion_solve_stats* out) { *out = state().stats; }
+
+int erosion_solve(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                  const double* yy, double* density, int64_t* nits) {
+  return guarded([&](State& s) {
+    Problem pr = make_problem(p, npts, nbods, nouter);
+    setup_from_host(s, pr, xx, yy);
+    const long long ntot = s.pr.ntot;
+    double* dd = s.d_den.ensure(ntot);
+    h2d(dd, density, ntot, s.st);
+    bool zero = true;
+    for (long long i = 0; i < ntot && zero; ++i) zero = density[i] == 0.0;
+    int rc = EROSION_OK;
+    try {
+      rc = solve_device_impl(s, dd, zero, nits);
+    } catch (const Error& e) {
+      if (e.code == EROSION_BAD_INPUT) {   // zero right-hand side: density zeroed
+        d2h(density, dd, ntot, s.st);
+        EB_CK(cudaStreamSynchronize(s.st));
+      }
+      throw;
+    }
+    d2h(density, dd, ntot, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    return rc;
+  });
+}
+
+int erosion_solve_device(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* d_xx,
+                         const double* d_yy, double* d_density, int64_t* nits) {
+  return guarded([&](State& s) {
+    Problem pr = make_problem(p, npts, nbods, nouter);
+    setup_problem(s, pr, d_xx, d_yy);
+    return solve_device_impl(s, d_density, false, nits);
+  });
+}
+
+void stokessolver_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter, const int64_t* ifmm,
+                   const int64_t* ibary, const int64_t* ibc, const int64_t* maxl, const double* xx, const double* yy,
+                   double* density, int64_t* nits) {
+  erosion_params p;
+  erosion_default_params(&p);
+  p.ifmm = (int32_t)*ifmm;
+  p.ibary = (int32_t)*ibary;
+  p.ibc = (int32_t)*ibc;
+  p.maxl = *maxl;
+  int64_t it = 0;
+  erosion_solve(&p, *npts, *nbods, *nouter, xx, yy, density, &it);
+  *nits = it;
+}
+
+int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                   const double* yy, const double* density, double* vel) {
+  return guarded([&](State& s) {
+    Problem pr = make_problem(p, npts, nbods, nouter);
+    setup_from_host(s, pr, xx, yy);
+    const long long ntot = s.pr.ntot;
+    double* dd = s.d_den.ensure(ntot);
+    double* dv = s.d_w.ensure(ntot);
+    h2d(dd, density, ntot, s.st);
+    apply_operator(s, dd, dv);
+    d2h(vel, dv, ntot, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    return EROSION_OK;
+  });
+}
+
+int erosion_rhs(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                const double* yy, double* rhs) {
+  return guarded([&](State& s) {
+    Problem pr = make_problem(p, npts, nbods, nouter);
+    setup_from_host(s, pr, xx, yy);
+    double* dr = s.d_rhs.ensure(s.pr.ntot);
+    build_rhs(s, dr);
+    d2h(rhs, dr, s.pr.ntot, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    return EROSION_OK;
+  });
+}
+
+int erosion_geometry(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                     const double* yy, double* px, double* py, double* cur, double* speed, double* cx, double* cy,
+                     double* xo, double* yo, double* px0, double* py0, double* cur0, double* speed0) {
+  return guarded([&](State& s) {
+    Problem pr = make_problem(p, npts, nbods, nouter);
+    setup_from_host(s, pr, xx, yy);
+    const int N = s.pr.N, nout = s.pr.nout, M = s.pr.M;
+    std::vector<double2> hxy(N), hn(N), hc(std::max(M, 1));
+    std::vector<double> hs(N), hk(N);
+    d2h(hxy.data(), s.xy.p, N, s.st);
+    d2h(hn.data(), s.nrm.p, N, s.st);
+    d2h(hs.data(), s.sp.p, N, s.st);
+    d2h(hk.data(), s.cur.p, N, s.st);
+    d2h(hc.data(), s.cen.p, M, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    for (int g = nout; g < N; ++g) {
+      int i = g - nout;
+      if (px) px[i] = hn[g].x;
+      if (py) py[i] = hn[g].y;
+      if (cur) cur[i] = hk[g];
+      if (speed) speed[i] = hs[g];
+    }
+    for (int b = 0; b < M; ++b) {
+      if (cx) cx[b] = hc[b].x;
+      if (cy) cy[b] = hc[b].y;
+    }
+    for (int g = 0; g < nout; ++g) {
+      if (xo) xo[g] = hxy[g].x;
+      if (yo) yo[g] = hxy[g].y;
+      if (px0) px0[g] = hn[g].x;
+      if (py0) py0[g] = hn[g].y;
+      if (cur0) cur0[g] = hk[g];
+      if (speed0) speed0[g] = hs[g];
+    }
+    return EROSION_OK;
+  });
+}
+
+int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (lw) *lw = s.near.lw;
+  if (wall_bodies)
+    for (size_t i = 0; i < s.near.wall_bodies.size(); ++i) wall_bodies[i] = s.near.wall_bodies[i];
+  if (near_pairs) *near_pairs = s.near.npairs;
+  return (int64_t)s.near.wall_bodies.size();
+}
+
+void erosion_release(void) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  DBuf<double>* dbs[] = {&s.dker_body, &s.dker_wall, &s.wx, &s.wy, &s.sp, &s.cur, &s.w, &s.rb, &s.sigdotn,
+                         &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.part, &s.hdev, &s.ydev};
+  for (auto* b : dbs) b->release();
+  DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.partial, &s.bd, &s.pair_out};
+  for (auto* b : d2s) b->release();
+  s.near.src_curve.release(); s.near.pair_tgt.release(); s.near.tptr.release(); s.near.tpairs.release();
+  s.near.bd_off.release(); s.near.bd_work.release(); s.near.bary_work.release(); s.near.mask.release();
+  s.tiles.release(); s.split_ptr.release();
+  s.vcap = 0;
+  s.dker_body_n = s.dker_wall_n = -1;
+  s.geo_valid = false;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// Host-side state of the library: device buffers kept between calls, the
+// current problem's geometry and near-field bookkeeping, and the status
+// channel of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <cstdint>
+#include <algorithm>
+#include "erosion_b200.h"
+#include "common.cuh"
+
+namespace eb {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define EB_CK(x)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess)                                                                     \
+      throw ::eb::Error(EROSION_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_));  \
+  } while (0)
+
+#define EB_LAUNCH_CHECK() EB_CK(cudaGetLastError())
+
+// Grow-only device buffer.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  T* ensure(size_t n) {
+    if (n > cap) {
+      release();
+      size_t m = std::max<size_t>(n, 1);
+      EB_CK(cudaMalloc((void**)&p, m * sizeof(T)));
+      cap = m;
+    }
+    return p;
+  }
+  // Grows keeping the first `keep` elements.
+  T* grow_keep(size_t n, size_t keep, cudaStream_t st) {
+    if (n <= cap) return p;
+    T* q = nullptr;
+    EB_CK(cudaMalloc((void**)&q, n * sizeof(T)));
+    if (p && keep) EB_CK(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    EB_CK(cudaStreamSynchronize(st));
+    release();
+    p = q;
+    cap = n;
+    return p;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+template <class T>
+void h2d(T* d, const T* h, size_t n, cudaStream_t st) {
+  if (n) EB_CK(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+template <class T>
+void d2h(T* h, const T* d, size_t n, cudaStream_t st) {
+  if (n) EB_CK(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+}
+
+inline unsigned nblk(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
+
+struct Problem {
+  int n = 0, M = 0, nout = 0, N = 0;
+  long long ntot = 0;
+  erosion_params P{};
+};
+
+// Near-field bookkeeping of one geometry.
+struct Near {
+  long long lw = 0;
+  std::vector<long long> wall_bodies;
+  int nsrc = 0;              // source curves with at least one pair
+  long long npairs = 0;
+  int mw = 0;                // mask words per target
+  int n_bd_work = 0, n_bary_work = 0;
+  long long bd_total = 0;    // complex entries of the boundary-value buffer
+  std::vector<int> h_src_curve, h_src_ptr, h_pair_tgt;
+  DBuf<int> src_curve, pair_tgt, tptr, tpairs;
+  DBuf<long long> bd_off;
+  DBuf<int2> bd_work;
+  DBuf<int4> bary_work;
+  DBuf<unsigned> mask;
+};
+
+struct State {
+  std::mutex mu;
+  int status = EROSION_OK;
+  std::string err;
+  bool init = false;
+  int device = -1;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, ef0 = nullptr, ef1 = nullptr;
+
+  Problem pr;
+  bool geo_valid = false;
+
+  // spectral derivative kernels
+  int dker_body_n = -1, dker_wall_n = -1;
+  DBuf<double> dker_body, dker_wall;
+
+  // geometry
+  DBuf<double> wx, wy, sp, cur, w, rb;
+  DBuf<double2> xy, nrm, dz, cen, d1tmp;
+
+  Near near;
+
+  // far field
+  DBuf<int4> tiles;
+  DBuf<int> split_ptr;
+  int nsplit = 0, ntile = 0;
+
+  // work buffers
+  DBuf<double2> ws, partial, bd, pair_out;
+  DBuf<double> sigdotn;
+  DBuf<double> d_xx, d_yy, d_den, d_rhs, d_r, d_w;
+
+  // Krylov
+  DBuf<double> V, part, hdev, ydev;
+  long long vcap = 0;   // vectors held by V
+  double* h_pinned = nullptr;
+  size_t h_pinned_cap = 0;
+
+  erosion_solve_stats stats{};
+
+  GeoDev geo() const {
+    GeoDev G;
+    G.n = pr.n; G.M = pr.M; G.nout = pr.nout; G.N = pr.N; G.ntot = pr.ntot;
+    G.xy = xy.p; G.nrm = nrm.p; G.sp = sp.p; G.cur = cur.p; G.w = w.p; G.dz = dz.p;
+    G.cen = cen.p; G.rb = rb.p;
+    return G;
+  }
+};
+
+State& state();
+void ensure_init(State& s);
+
+// Geometry + near lists + far-field tiles for (xx, yy) already on the device.
+void setup_problem(State& s, const Problem& pr, const double* d_xx, const double* d_yy);
+// vel = A den (FP64 operator), device pointers.
+void apply_operator(State& s, const double* d_den, double* d_vel);
+void build_rhs(State& s, double* d_rhs);
+// GMRES (SLATEC DGMRES semantics, CGS2 Arnoldi); returns EROSION_* status.
+int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
+                long long* iters, double* est);
+double device_norm(State& s, const double* d_v, long long n);
+
+// Shear stress / targets (stress.cu)
+void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E);
+void qoi_targets(State& s, const double* d_den, long long ntar, const double* d_xt, const double* d_yt,
+                 double* d_u, double* d_v, double* d_p, double* d_w);
+
+}  // namespace eb

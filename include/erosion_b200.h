@@ -1,0 +1,174 @@
+/*
+ * erosion_b200 — C ABI of the B200 Stokes boundary-integral library.
+ *
+ * The first three entry points keep the names, argument order and by-reference
+ * convention of the Fortran routines that quaife/erosion's Julia package binds
+ * with `ccall` from `libstokes.so`, so the library drops in for that file.
+ * Integer arguments are int64 (Julia's `Ref{Int}`); every array is caller
+ * owned host memory and is final when the call returns.  Calls are serialised
+ * by an internal mutex; the library keeps its device buffers between calls.
+ *
+ * Unknown layout (the reference's, stokesSolver.f:469-470, :636-660, :993-995):
+ *   [ wall sigma_x (nouter) | wall sigma_y (nouter) |
+ *     per body b: sigma_x (npts), sigma_y (npts) |
+ *     per body b: stokeslet_x, stokeslet_y, rotlet ]
+ *   length 2*nouter + 2*npts*nbods + 3*nbods.
+ *
+ * Errors: the reference has no error channel (its subroutines return nothing
+ * and ignore DGMRES's IERR).  These entry points keep `void` and record an
+ * outcome readable through erosion_last_status()/erosion_last_error().
+ */
+#ifndef EROSION_B200_H
+#define EROSION_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum {
+  EROSION_OK = 0,            /* converged / completed                          */
+  EROSION_MAXITER = 1,       /* GMRES reached maxl without meeting tol         */
+  EROSION_BREAKDOWN = 2,     /* GMRES stalled, or a NaN/Inf appeared           */
+  EROSION_BAD_INPUT = 3,     /* sizes, geometry or arguments rejected          */
+  EROSION_CUDA_ERROR = 4,    /* a CUDA call failed                             */
+  EROSION_NO_DEVICE = 5      /* no usable CUDA device                          */
+};
+
+/* Replaces stokesSolver (ErosionPackage/fortran_code/stokesSolver.f:1-131),
+ * bound at ErosionPackage/src/DensityStress.jl:48-51.  Builds the geometry and
+ * right-hand side, then solves the double-layer boundary integral equation by
+ * unrestarted GMRES to relative residual 1e-8.  density is the initial guess
+ * on entry and the solution on exit; nits receives the GMRES iterations.
+ * ifmm is accepted for ABI compatibility: the far field is an exact direct sum.
+ * ibary = 1 applies the barycentric near-singular corrections with the
+ * selection rules of matvec_DLP_fmmbary (ifmm = 1) or to every pair of
+ * distinct curves as matvec_DLP_bary does (ifmm = 0); ibary = 0 is the
+ * trapezoid rule everywhere.  ibc = 0 parabolic, 1 uniform wall velocity. */
+void stokessolver_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter,
+                   const int64_t* ifmm, const int64_t* ibary, const int64_t* ibc,
+                   const int64_t* maxl, const double* xx, const double* yy,
+                   double* density, int64_t* nits);
+
+/* Replaces computeShearStress (stokesSolver.f:3002-3096), bound at
+ * DensityStress.jl:195-198.  tau[npts*nbods] receives the wall shear stress on
+ * every body node; ibary = 1 evaluates other curves' contributions with the
+ * barycentric formulas (deformation_on_boundary), 0 with the trapezoid rule
+ * (deformation_on_boundary_trap). */
+void computeshearstress_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter,
+                         const double* xx, const double* yy, const double* density,
+                         const int64_t* ibary, double* tau);
+
+/* Replaces computeQoiTargets (stokesSolver.f:3099-3323), bound at
+ * DensityStress.jl:81-86: velocity, pressure and vorticity at ntargets points;
+ * targets classified inside a body are zeroed. */
+void computeqoitargets_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter,
+                        const int64_t* ibary, const double* xx, const double* yy,
+                        const double* density, const int64_t* ntargets,
+                        const double* xtar, const double* ytar, double* utar,
+                        double* vtar, double* ptar, double* vortar);
+
+/* Outcome of the last call on this process (EROSION_* code) and a message. */
+int erosion_last_status(void);
+const char* erosion_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Extended interface (no counterpart in the reference's ABI): the knobs the
+ * reference hard-codes, precision mode, device-resident operands, and the
+ * pieces the parity tests compare one by one.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  double wall_a;        /* wall semi-axis in x (reference 3, stokesSolver.f:189)   */
+  double wall_b;        /* wall semi-axis in y (reference 1, :190); also the channel
+                           half-height used by the near-wall tests (:717-719, 769)
+                           and by the parabolic wall data (:398-404)               */
+  double wall_order;    /* superellipse order (reference 8, :186)                  */
+  double tol;           /* GMRES relative residual (reference 1e-8, :482)          */
+  int64_t maxl;         /* iteration cap (reference ParamSet maxl = 8000)          */
+  int32_t ibary;        /* 1 barycentric near field, 0 trapezoid                   */
+  int32_t ifmm;         /* with ibary=1: 1 fmmbary selection rules, 0 all pairs    */
+  int32_t ibc;          /* 0 parabolic, 1 uniform wall velocity                    */
+  int32_t precision;    /* 0 FP64; 1 mixed: FP32 compensated far field inside FP64
+                           iterative refinement to the same tol                    */
+  int32_t rhs_mode;     /* 0 production data; 1 the reference's manufactured
+                           stokeslet (1,2) + rotlet 3 at the origin (:220-257);
+                           2 homogeneous (all-zero) data                           */
+  int32_t true_residual;/* 1: also evaluate ||b - A x||/||b|| with the FP64 operator */
+  int32_t reserved[6];
+} erosion_params;
+
+/* Fills the reference's defaults: wall (3, 1, 8), tol 1e-8, maxl 8000, ibary 1,
+ * ifmm 1, ibc 1, FP64, production right-hand side. */
+void erosion_default_params(erosion_params* p);
+
+/* Solve statistics of the last erosion_solve / stokessolver_ call. */
+typedef struct {
+  int64_t iterations;       /* GMRES iterations (sum over refinement sweeps)       */
+  int64_t matvecs;          /* operator applications, all precisions               */
+  int64_t matvecs_fp32;     /* of which with the FP32 far field                    */
+  int64_t sweeps;           /* outer refinement sweeps (1 for FP64)                */
+  double est_residual;      /* GMRES estimate rho/||b|| at exit                    */
+  double true_residual;     /* ||b - A x||/||b|| (FP64 operator) when requested    */
+  double ms_total;          /* device time of the solve                            */
+  double ms_far;            /* device time inside the far-field kernel             */
+  int64_t far_launches;     /* far-field kernel launches                           */
+  int64_t near_pairs;       /* (target node, source curve) barycentric pairs       */
+} erosion_solve_stats;
+
+/* Host-array solve.  density: initial guess in, solution out. */
+int erosion_solve(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                  const double* xx, const double* yy, double* density, int64_t* nits);
+
+/* Same with device pointers (inputs resident in HBM; density updated in place). */
+int erosion_solve_device(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                         const double* d_xx, const double* d_yy, double* d_density, int64_t* nits);
+
+void erosion_get_solve_stats(erosion_solve_stats* s);
+
+/* One application of the boundary operator (host arrays) — the reference's
+ * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm. */
+int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                   const double* xx, const double* yy, const double* density, double* vel);
+
+/* The right-hand side of bd_condition (stokesSolver.f:208-314). */
+int erosion_rhs(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                const double* xx, const double* yy, double* rhs);
+
+/* Geometry as compute_derivs/inner_geometry/outer_geometry build it; any
+ * output may be NULL.  Body arrays npts*nbods, per-body nbods, wall nouter. */
+int erosion_geometry(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                     const double* xx, const double* yy, double* px, double* py, double* cur,
+                     double* speed, double* cx, double* cy, double* xo, double* yo,
+                     double* px0, double* py0, double* cur0, double* speed0);
+
+/* Shear stress (host arrays); E, if not NULL, receives E11, E12, E22 (3*npts*nbods). */
+int erosion_shear_stress(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                         const double* xx, const double* yy, const double* density,
+                         double* tau, double* E);
+
+int erosion_shear_stress_device(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                                const double* d_xx, const double* d_yy, const double* d_density,
+                                double* d_tau);
+
+/* Velocity, pressure, vorticity at targets (host arrays). */
+int erosion_qoi_targets(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                        const double* xx, const double* yy, const double* density,
+                        int64_t ntargets, const double* xtar, const double* ytar,
+                        double* utar, double* vtar, double* ptar, double* vortar);
+
+/* Near-pair bookkeeping of the last geometry set up: the integer wall length
+ * scale 'lw' of matvec_DLP_fmmbary (an INTEGER there, :705-709), the number
+ * of near-wall bodies (written to wall_bodies, capacity nbods) and the total
+ * number of barycentric (target node, source curve) pairs. */
+int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs);
+
+/* Releases every device buffer the library holds. */
+void erosion_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EROSION_B200_H */

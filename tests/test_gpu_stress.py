@@ -1,0 +1,89 @@
+"""GPU parity of the shear stress (computeShearStress) and the target
+quantities (computeQoiTargets) against the CPU FP64 oracle, through the C ABI.
+Tolerance: 1e-9 relative (max norm) for the shear stress and the deformation
+tensor, 1e-10 for the target quantities."""
+import numpy as np
+import pytest
+
+from erosion_b200 import geometry as G
+from erosion_b200 import stokes
+
+pytestmark = pytest.mark.gpu
+
+TAU_RTOL = 1e-9
+QOI_RTOL = 1e-10
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def small():
+    return G.workload("ref-small")
+
+
+@pytest.fixture(scope="module")
+def small_den(oracle, small):
+    den, nits, ierr, err = oracle.solve(small, tol=1e-12)
+    return den
+
+
+@pytest.mark.parametrize("ibary", [1, 0])
+def test_shear_stress_matches_oracle(lib, oracle, small, small_den, ibary):
+    tau, E = stokes.shear_stress(small, small_den, ibary=ibary)
+    tau_o, E_o = oracle.shear_stress(small, small_den, ibary=ibary)
+    assert rel(tau, tau_o) < TAU_RTOL
+    for q in range(3):
+        assert rel(E[q], E_o[q]) < TAU_RTOL
+
+
+def test_shear_stress_random_density(lib, oracle, small):
+    den = np.random.default_rng(7).standard_normal(small.ntot)
+    tau, _ = stokes.shear_stress(small, den)
+    tau_o, _ = oracle.shear_stress(small, den)
+    assert rel(tau, tau_o) < TAU_RTOL
+
+
+def test_shear_stress_channel_c1(lib, oracle):
+    g = G.workload("c1", seed=1)
+    den = np.random.default_rng(3).standard_normal(g.ntot)
+    tau, _ = stokes.shear_stress(g, den)
+    tau_o, _ = oracle.shear_stress(g, den)
+    assert rel(tau, tau_o) < TAU_RTOL
+
+
+def test_shear_stress_abi_entry(lib, oracle, small, small_den):
+    """computeshearstress_ (the drop-in symbol, by-reference int64 args)."""
+    import ctypes
+    from erosion_b200._lib import PD, PI64
+    tau = np.zeros(small.n * small.M)
+    i = lambda v: ctypes.byref(ctypes.c_int64(v))
+    # the drop-in uses the reference wall
+    lib.computeshearstress_(i(small.n), i(small.M), i(small.nout), small.xx.ctypes.data_as(PD),
+                            small.yy.ctypes.data_as(PD), small_den.ctypes.data_as(PD), i(1),
+                            tau.ctypes.data_as(PD))
+    tau_o, _ = oracle.shear_stress(small, small_den)
+    assert rel(tau, tau_o) < TAU_RTOL
+
+
+@pytest.mark.parametrize("ibary", [1, 0])
+def test_qoi_targets_matches_oracle(lib, oracle, small, small_den, ibary):
+    ylocs = -1 + (np.arange(13) + 0.5) * 2 / 13
+    xt = np.r_[np.full(13, 2.0), np.full(13, -2.0), [-1.0, 0.6, 1.5]]   # last: inside, inside, fluid
+    yt = np.r_[ylocs, ylocs, [0.1, 0.72, 0.3]]
+    a = stokes.qoi_targets(small, small_den, xt, yt, ibary=ibary)
+    b = oracle.qoi_targets(small, small_den, xt, yt, ibary=ibary)
+    for q in range(4):
+        assert rel(a[q], b[q]) < QOI_RTOL, q
+    assert a[0][26] == 0.0 and a[0][27] == 0.0    # inside bodies are zeroed
+    assert a[0][28] != 0.0
+
+
+def test_pressure_drop_flux_consistency(lib, small):
+    """DensityStress.jl:149-152: the flux through x = +-x0 must agree."""
+    den, _, _ = stokes.solve(small, tol=1e-10)
+    ylocs = -1 + (np.arange(13) + 0.5) * 2 / 13
+    up = stokes.qoi_targets(small, den, np.full(13, 2.0), ylocs)[0]
+    um = stokes.qoi_targets(small, den, np.full(13, -2.0), ylocs)[0]
+    assert abs(up.mean() - um.mean()) / abs(0.5 * (up.mean() + um.mean())) < 1e-3
