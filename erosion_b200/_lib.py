@@ -75,6 +75,27 @@ class SolveStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class StepParams(ctypes.Structure):
+    """Mirror of ``erosion_step_params``."""
+
+    _fields_ = [("dt", c_double), ("epsilon", c_double), ("sigma", c_double),
+                ("fixarea", c_int32), ("fixpdrop", c_int32), ("warm_start", c_int32),
+                ("reserved", c_int32 * 5)]
+
+
+class StepStats(ctypes.Structure):
+    """Mirror of ``erosion_step_stats``."""
+
+    _fields_ = [("gmres_iterations", c_int64 * 2), ("bodies_deleted", c_int64),
+                ("ms_solve", c_double), ("ms_stress", c_double), ("ms_thetalen", c_double),
+                ("ms_total", c_double), ("max_residual", c_double), ("matau", c_double * 2)]
+
+    def as_dict(self) -> dict:
+        return {"gmres_iterations": list(self.gmres_iterations), "bodies_deleted": self.bodies_deleted,
+                "ms_solve": self.ms_solve, "ms_stress": self.ms_stress, "ms_thetalen": self.ms_thetalen,
+                "ms_total": self.ms_total, "max_residual": self.max_residual, "matau": list(self.matau)}
+
+
 # Every entry point declared in include/erosion_b200.h, with its signature.
 SIGNATURES = {
     "stokessolver_": (None, [PI64] * 7 + [PD, PD, PD, PI64]),
@@ -96,6 +117,17 @@ SIGNATURES = {
     "erosion_qoi_targets": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, c_int64,
                                     PD, PD, PD, PD, PD, PD]),
     "erosion_near_info": (c_int64, [PI64, PI64, PI64]),
+    "erosion_default_step_params": (None, [POINTER(StepParams), c_int64]),
+    "erosion_get_step_stats": (None, [POINTER(StepStats)]),
+    "erosion_rk2_step": (c_int, [POINTER(ErosionParams), POINTER(StepParams), c_int64, PI64, c_int64,
+                                 PD, PD, PD, PD, PD, PI64]),
+    "erosion_rk2_step_device": (c_int, [POINTER(ErosionParams), POINTER(StepParams), c_int64, PI64, c_int64,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        PD, PI64]),
+    "erosion_getxy": (c_int, [c_int64, c_int64, PD, PD, PD, PD, PD, PD]),
+    "erosion_stream": (ctypes.c_void_p, []),
+    "erosion_launch_count": (c_int64, []),
+    "erosion_peak_tflops": (c_double, [c_int32]),
     "erosion_release": (None, []),
 }
 

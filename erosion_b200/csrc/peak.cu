@@ -1,0 +1,63 @@
+// FMA throughput microbenchmark: the denominator of the pair kernels'
+// roofline (FP64 or FP32 vector pipe; the far field is not a contraction).
+#include "state.h"
+
+namespace {
+
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters, T a, T b) {
+  T x0 = (T)threadIdx.x, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3;
+  T x4 = x0 + (T)4, x5 = x0 + (T)5, x6 = x0 + (T)6, x7 = x0 + (T)7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  T r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (r == (T)-12345) out[0] = r;   // keeps the chains alive
+}
+
+}  // namespace
+
+using namespace eb;
+
+extern "C" double erosion_peak_tflops(int32_t precision) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  try {
+    ensure_init(s);
+    cudaDeviceProp prop;
+    EB_CK(cudaGetDeviceProperties(&prop, s.device));
+    const int blocks = prop.multiProcessorCount * 8, threads = 256;
+    static DBuf<double> sink;
+    sink.ensure(1);
+    cudaEvent_t a, b;
+    EB_CK(cudaEventCreate(&a));
+    EB_CK(cudaEventCreate(&b));
+    const int iters = precision == 0 ? 2048 : 4096;
+    double best = 0;
+    for (int rep = 0; rep < 4; ++rep) {
+      EB_CK(cudaEventRecord(a, s.st));
+      if (precision == 0)
+        k_fma_peak<double><<<blocks, threads, 0, s.st>>>(sink.p, iters, 0.999999, 1e-7);
+      else
+        k_fma_peak<float><<<blocks, threads, 0, s.st>>>((float*)sink.p, iters, 0.999999f, 1e-7f);
+      EB_LAUNCH_CHECK();
+      EB_CK(cudaEventRecord(b, s.st));
+      EB_CK(cudaEventSynchronize(b));
+      float ms = 0;
+      EB_CK(cudaEventElapsedTime(&ms, a, b));
+      double flops = 2.0 * 64.0 * iters * (double)blocks * threads;
+      if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return best;
+  } catch (const Error& e) {
+    s.status = e.code;
+    s.err = e.what();
+    return -1.0;
+  }
+}

@@ -12,6 +12,7 @@ State& state() {
   return s;
 }
 
+long long g_launches = 0;
 static int g_num_sms = 148;
 int eb_num_sms() { return g_num_sms; }
 
@@ -255,7 +256,17 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   s.geo_valid = true;
 }
 
+void harvest_far_timing(State& s) {
+  if (!s.far_pending) return;
+  float ms = 0;
+  EB_CK(cudaEventSynchronize(s.ef1));   // complete already on every path that calls this
+  EB_CK(cudaEventElapsedTime(&ms, s.ef0, s.ef1));
+  s.stats.ms_far += ms;
+  s.far_pending = false;
+}
+
 void apply_operator(State& s, const double* d_den, double* d_vel) {
+  harvest_far_timing(s);
   const Problem& pr = s.pr;
   const GeoDev G = s.geo();
   const Near& nr = s.near;
@@ -270,6 +281,7 @@ void apply_operator(State& s, const double* d_den, double* d_vel) {
     k_far64<false><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nullptr, 0, s.partial.p);
   EB_LAUNCH_CHECK();
   EB_CK(cudaEventRecord(s.ef1, st));
+  s.far_pending = true;
   if (nr.npairs > 0) {
     k_bdval<<<nr.n_bd_work, BD_NT, 0, st>>>(G, d_den, nr.bd_work.p, nr.src_curve.p, nr.bd_off.p, s.dker_wall.p,
                                             s.dker_body.p, s.bd.p);
@@ -405,6 +417,7 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
     std::vector<double> h2h(k);
     d2h(h2h.data(), hs, (size_t)k, st);
     EB_CK(cudaStreamSynchronize(st));
+    harvest_far_timing(s);
     const double snormw = std::sqrt(hp[k]);
     std::vector<double> col(ll + 1);
     for (int i = 0; i < k; ++i) col[i] = hp[i] + h2h[i];
@@ -534,6 +547,7 @@ int solve_device_impl(State& s, double* d_den, bool x0_zero, int64_t* nits) {
   }
   EB_CK(cudaEventRecord(s.e1, s.st));
   EB_CK(cudaEventSynchronize(s.e1));
+  harvest_far_timing(s);
   float ms = 0;
   EB_CK(cudaEventElapsedTime(&ms, s.e0, s.e1));
   s.stats.ms_total = ms;
@@ -680,6 +694,21 @@ int erosion_geometry(const erosion_params* p, int64_t npts, int64_t nbods, int64
     return EROSION_OK;
   });
 }
+
+void* erosion_stream(void) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  try {
+    ensure_init(s);
+  } catch (const Error& e) {
+    s.status = e.code;
+    s.err = e.what();
+    return nullptr;
+  }
+  return (void*)s.st;
+}
+
+int64_t erosion_launch_count(void) { return (int64_t)g_launches; }
 
 int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs) {
   State& s = state();

@@ -14,6 +14,8 @@
 
 namespace eb {
 
+extern long long g_launches;
+
 struct Error : std::runtime_error {
   int code;
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
@@ -26,7 +28,11 @@ struct Error : std::runtime_error {
       throw ::eb::Error(EROSION_CUDA_ERROR, std::string(#x) + ": " + cudaGetErrorString(e_));  \
   } while (0)
 
-#define EB_LAUNCH_CHECK() EB_CK(cudaGetLastError())
+#define EB_LAUNCH_CHECK()  \
+  do {                     \
+    ++::eb::g_launches;    \
+    EB_CK(cudaGetLastError()); \
+  } while (0)
 
 // Grow-only device buffer.
 template <class T>
@@ -134,6 +140,7 @@ struct State {
   size_t h_pinned_cap = 0;
 
   erosion_solve_stats stats{};
+  bool far_pending = false;   // ef0/ef1 bracket a far-field launch not yet harvested
 
   GeoDev geo() const {
     GeoDev G;
@@ -156,6 +163,8 @@ void build_rhs(State& s, double* d_rhs);
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
                 long long* iters, double* est);
 double device_norm(State& s, const double* d_v, long long n);
+// Adds the last far-field launch's event time to stats.ms_far (after a sync).
+void harvest_far_timing(State& s);
 
 // Shear stress / targets (stress.cu)
 void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E);

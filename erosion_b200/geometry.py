@@ -177,3 +177,21 @@ def custom(n: int, nout: int, radii, centers, wall=REFERENCE_WALL, ibc: int = 1)
     centers = np.asarray(centers, float).reshape(-1, 2)
     xx, yy = make_bodies(n, radii, centers)
     return Geometry(n, nout, xx, yy, tuple(wall), ibc, radii, centers)
+
+
+def to_thetalen(g: Geometry):
+    """theta-L state (theta [M*n], L [M], xsm [M], ysm [M]) of body-major nodes
+    sampled at equal arclength on the offset grid: theta is the tangent angle
+    (unwrapped, theta - alpha periodic), L the perimeter, (xsm, ysm) the
+    surface mean (ThetaLen.jl:42-51)."""
+    n, M = g.n, g.M
+    x = g.xx.reshape(M, n)
+    y = g.yy.reshape(M, n)
+    k = np.fft.fftfreq(n, 1.0 / n)
+    k[n // 2] = 0.0
+    dx = np.real(np.fft.ifft(1j * k * np.fft.fft(x, axis=1), axis=1))
+    dy = np.real(np.fft.ifft(1j * k * np.fft.fft(y, axis=1), axis=1))
+    th = np.unwrap(np.arctan2(dy, dx), axis=1)
+    L = np.mean(np.hypot(dx, dy), axis=1) * 2 * np.pi
+    return (np.ascontiguousarray(th.reshape(-1)), np.ascontiguousarray(L), np.ascontiguousarray(x.mean(1)),
+            np.ascontiguousarray(y.mean(1)))

@@ -164,6 +164,76 @@ int erosion_qoi_targets(const erosion_params* p, int64_t npts, int64_t nbods, in
  * number of barycentric (target node, source curve) pairs. */
 int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs);
 
+/* ------------------------------------------------------------------------
+ * Erosion time step (theta-L form).  Replaces the Julia time loop's step
+ * rungekutta2 (ErosionPackage/src/TimeStepping.jl:189-202) with everything it
+ * calls: getxy (ThetaLen.jl:92-101), getstress! (DensityStress.jl:23-36,
+ * i.e. the solve, the optional fixed-pressure-drop rescale and the shear
+ * stress), getderivs (TimeStepping.jl:63-95), delete_indices (:103-126) and
+ * timestep! (:130-185), all on the device.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  double dt;            /* time step (ParamSet dt, ThetaLen.jl:27)               */
+  double epsilon;       /* curvature smoothing (epsfac/npts)                     */
+  double sigma;         /* stress smoothing (sigfac/npts)                        */
+  int32_t fixarea;      /* ParamSet fixarea                                      */
+  int32_t fixpdrop;     /* ParamSet fixpdrop: rescale the density so that the
+                           pressure drop between x = -2 and x = 2 is 8
+                           (DensityStress.jl:129-167; meaningful for walls
+                           that contain those slices)                            */
+  int32_t warm_start;   /* 0: zero initial guess (the reference,
+                           DensityStress.jl:45); 1: previous solve's density of
+                           the same stage when the body count is unchanged       */
+  int32_t reserved[5];
+} erosion_step_params;
+
+/* Fills the ParamSet defaults for npts: dt 1e-3, epsilon 15/npts,
+ * sigma 10/npts, fixarea 0, fixpdrop 1, warm_start 0. */
+void erosion_default_step_params(erosion_step_params* sp, int64_t npts);
+
+/* Per-step statistics of the last erosion_rk2_step call. */
+typedef struct {
+  int64_t gmres_iterations[2];  /* per stage                                  */
+  int64_t bodies_deleted;
+  double ms_solve;              /* device time in the two solves              */
+  double ms_stress;             /* device time in the two shear stresses      */
+  double ms_thetalen;           /* device time in the theta-L arithmetic      */
+  double ms_total;
+  double max_residual;          /* largest GMRES estimate at exit             */
+  double matau[2];              /* mean smoothed |tau| over bodies, per stage */
+} erosion_step_stats;
+
+/* One RK2 step of the theta-L state, host arrays, in place:
+ * theta[nbods*npts], len/xsm/ysm[nbods]; *nbods is updated when bodies are
+ * deleted and deleted[] (capacity nbods) receives their original indices.
+ * *t is advanced by dt. */
+int erosion_rk2_step(const erosion_params* p, const erosion_step_params* sp, int64_t npts,
+                     int64_t* nbods, int64_t nouter, double* theta, double* len, double* xsm,
+                     double* ysm, double* t, int64_t* deleted);
+
+/* Same with the state resident on the device (in place). */
+int erosion_rk2_step_device(const erosion_params* p, const erosion_step_params* sp, int64_t npts,
+                            int64_t* nbods, int64_t nouter, double* d_theta, double* d_len,
+                            double* d_xsm, double* d_ysm, double* t, int64_t* deleted);
+
+void erosion_get_step_stats(erosion_step_stats* s);
+
+/* Node coordinates of theta-L bodies (getxy, ThetaLen.jl:92-101), host arrays. */
+int erosion_getxy(int64_t npts, int64_t nbods, const double* theta, const double* len,
+                  const double* xsm, const double* ysm, double* xx, double* yy);
+
+/* The CUDA stream every library kernel is launched on (a cudaStream_t), so a
+ * caller can order its own work and events with the library's. */
+void* erosion_stream(void);
+
+/* Number of kernels the library has launched since the process started. */
+int64_t erosion_launch_count(void);
+
+/* Measured vector FMA throughput of this GPU in TFLOP/s (2 flops per FMA):
+ * precision 0 = FP64, 1 = FP32, from a ~10 ms register-resident FMA loop
+ * over every SM (the roofline denominator of the pair kernels). */
+double erosion_peak_tflops(int32_t precision);
+
 /* Releases every device buffer the library holds. */
 void erosion_release(void);
 
