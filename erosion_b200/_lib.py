@@ -51,7 +51,9 @@ class ErosionParams(ctypes.Structure):
         ("precision", c_int32),
         ("rhs_mode", c_int32),
         ("true_residual", c_int32),
-        ("reserved", c_int32 * 6),
+        ("precond", c_int32),
+        ("reserved", c_int32 * 5),
+        ("relax_tol", c_double),
     ]
 
 
@@ -69,6 +71,10 @@ class SolveStats(ctypes.Structure):
         ("ms_far", c_double),
         ("far_launches", c_int64),
         ("near_pairs", c_int64),
+        ("ms_far32", c_double),
+        ("far32_launches", c_int64),
+        ("far32_pairs", c_int64),
+        ("true_residual_checks", c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -11,6 +11,7 @@ namespace {
 constexpr int FAR_NT = 256;        // threads per CTA
 constexpr int FAR_TPT = 2;         // targets per thread (FP64)
 constexpr int FAR_TS = 256;        // sources per shared-memory tile (<= FAR_NT)
+constexpr int WALL_TS = 32;        // wall nodes per tile (keeps FP32 offsets small)
 constexpr int NEAR_NT = 128;       // threads per CTA of the barycentric kernels
 constexpr int NEAR_TK = 128;       // source nodes per shared-memory tile
 constexpr int BD_NT = 256;         // threads per CTA of the boundary-value kernel
@@ -215,6 +216,415 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
     int i = i0 + q * FAR_NT;
     if (i < N) partial[(size_t)split * N + i] = make_double2(ax[q], ay[q]);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Far field, FP32 with compensated accumulation (the mixed-precision operator).
+// Same sum as k_far64 but over pairs of DIFFERENT curves only (a target's own
+// curve is evaluated in FP64 by k_self64) and without the near-masked pairs.
+// Each 256-source tile is summed in FP32 and folded into a two-sum (Knuth)
+// accumulator (hi, lo), so the rounding error grows with the tile length, not
+// with N.  Positions are absolute FP32 coordinates; the excluded pairs are
+// exactly the close ones where that would lose accuracy.
+constexpr int F32_NT = 256;
+constexpr int F32_TPT = 4;
+constexpr int F32_TS = 256;
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t) {
+  float s = hi + t;
+  float bp = s - hi;
+  float e = (hi - (s - bp)) + (t - bp);
+  hi = s;
+  lo += e;
+}
+
+template <bool MASK>
+__global__ void __launch_bounds__(F32_NT, 2)
+k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
+        const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+        const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
+        double2* __restrict__ partial) {
+  // Every node is stored as an FP32 offset from the FP64 centre of its own
+  // tile (tiles never cross a curve and are at most one body or 32 wall nodes
+  // long).  Per (target, source tile) the centre difference is formed in
+  // FP64, so r = (c_t - c_s) + (o_t - o_s) is rounded relative to |r|, not to
+  // the magnitude of the coordinates.
+  __shared__ float4 sg[F32_TS];
+  __shared__ float2 sw[F32_TS];
+  const int split = blockIdx.y;
+  const int i0 = blockIdx.x * (F32_NT * F32_TPT) + threadIdx.x;
+  int it[F32_TPT], cv[F32_TPT];
+  double ax[F32_TPT], ay[F32_TPT];
+  float ox[F32_TPT], oy[F32_TPT], hx[F32_TPT], lx[F32_TPT], hy[F32_TPT], ly[F32_TPT];
+#pragma unroll
+  for (int q = 0; q < F32_TPT; ++q) {
+    int i = i0 + q * F32_NT;
+    it[q] = i < N ? i : N - 1;
+    cv[q] = it[q] < nout ? 0 : 1 + (it[q] - nout) / n;
+    float2 p = tgt[it[q]];
+    double2 a = anchor[it[q]];
+    ox[q] = p.x; oy[q] = p.y; ax[q] = a.x; ay[q] = a.y;
+    hx[q] = lx[q] = hy[q] = ly[q] = 0.f;
+  }
+  const int tb = split_ptr[split], te = split_ptr[split + 1];
+  for (int ti = tb; ti < te; ++ti) {
+    const int4 T = tiles[ti];
+    __syncthreads();
+    if (threadIdx.x < T.y) {
+      sg[threadIdx.x] = src[T.x + threadIdx.x];
+      sw[threadIdx.x] = ws32[T.x + threadIdx.x];
+    }
+    __syncthreads();
+    const double2 cs = tile_c[ti];
+    float px[F32_TPT], py[F32_TPT], tx[F32_TPT], ty[F32_TPT];
+#pragma unroll
+    for (int q = 0; q < F32_TPT; ++q) {
+      px[q] = (float)(ax[q] - cs.x) + ox[q];
+      py[q] = (float)(ay[q] - cs.y) + oy[q];
+      tx[q] = 0.f;
+      ty[q] = 0.f;
+    }
+#pragma unroll 4
+    for (int j = 0; j < T.y; ++j) {
+      const float4 s = sg[j];
+      const float2 a = sw[j];
+#pragma unroll
+      for (int q = 0; q < F32_TPT; ++q) {
+        float rx = px[q] - s.x, ry = py[q] - s.y;
+        float rho2 = fmaf(rx, rx, ry * ry);
+        float rdn = fmaf(rx, s.z, ry * s.w);
+        float rds = fmaf(rx, a.x, ry * a.y);
+        float inv = rcp_approx(rho2);
+        float c = (rdn * rds) * (inv * inv);
+        tx[q] = fmaf(c, rx, tx[q]);
+        ty[q] = fmaf(c, ry, ty[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < F32_TPT; ++q) {
+      bool use = T.z != cv[q];
+      if (MASK) use = use && !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
+      if (use) { two_sum_add(hx[q], lx[q], tx[q]); two_sum_add(hy[q], ly[q], ty[q]); }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < F32_TPT; ++q) {
+    int i = i0 + q * F32_NT;
+    if (i < N) partial[(size_t)split * N + i] = make_double2((double)hx[q] + (double)lx[q], (double)hy[q] + (double)ly[q]);
+  }
+}
+
+// Tile centres (middle node) and, per node, the FP32 offset from its tile's
+// centre plus that centre (the target anchor of k_far32).  One CTA per tile.
+__global__ void k_geom32(int ntile, const int4* __restrict__ tiles, const double2* __restrict__ xy,
+                         const double2* __restrict__ nrm, double2* __restrict__ tile_c, float4* __restrict__ src,
+                         float2* __restrict__ tgt, double2* __restrict__ anchor) {
+  const int t = blockIdx.x;
+  if (t >= ntile) return;
+  const int4 T = tiles[t];
+  const double2 c = xy[T.x + T.y / 2];
+  if (threadIdx.x == 0) tile_c[t] = c;
+  for (int k = threadIdx.x; k < T.y; k += blockDim.x) {
+    int g = T.x + k;
+    double2 p = xy[g], nn = nrm[g];
+    float ox = (float)(p.x - c.x), oy = (float)(p.y - c.y);
+    src[g] = make_float4(ox, oy, (float)nn.x, (float)nn.y);
+    tgt[g] = make_float2(ox, oy);
+    anchor[g] = c;
+  }
+}
+
+// FP64 pairs within each curve (i != j): the self-interaction part of the
+// far-field sum for the mixed-precision operator.  CTA = (curve, <=256
+// targets); the curve streams through shared memory.
+__global__ void __launch_bounds__(256)
+k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tasks, double2* __restrict__ out) {
+  __shared__ double4 sg[256];
+  __shared__ double2 sw[256];
+  const int4 tk = tasks[blockIdx.x];   // target start, count, curve
+  const int c = tk.z;
+  const int start = curve_start(G, c), len = curve_len(G, c);
+  const int i = tk.x + threadIdx.x;
+  const bool act = threadIdx.x < tk.y;
+  const int ic = act ? i : tk.x;
+  const double2 p = G.xy[ic];
+  double ax = 0.0, ay = 0.0;
+  for (int k0 = 0; k0 < len; k0 += 256) {
+    __syncthreads();
+    const int kl = k0 + threadIdx.x;
+    if (kl < len) {
+      int g = start + kl;
+      double2 q = G.xy[g], nn = G.nrm[g];
+      sg[threadIdx.x] = make_double4(q.x, q.y, nn.x, nn.y);
+      sw[threadIdx.x] = ws[g];
+    }
+    __syncthreads();
+    const int kt = min(256, len - k0);
+    for (int j = 0; j < kt; ++j) {
+      const double4 s = sg[j];
+      const double2 a = sw[j];
+      double rx = p.x - s.x, ry = p.y - s.y;
+      double rho2 = fma(rx, rx, ry * ry);
+      double rdn = fma(rx, s.z, ry * s.w);
+      double rds = fma(rx, a.x, ry * a.y);
+      double inv = rcp_or_zero(rho2);
+      double cc = rdn * rds * inv * inv;
+      ax = fma(cc, rx, ax);
+      ay = fma(cc, ry, ay);
+    }
+  }
+  if (act) out[i] = make_double2(ax, ay);
+}
+
+__global__ void k_ws32(int N, const double2* __restrict__ ws, float2* __restrict__ out) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N) return;
+  double2 a = ws[g];
+  out[g] = make_float2((float)a.x, (float)a.y);
+}
+
+// ---------------------------------------------------------------------------
+// Block Gauss-Seidel preconditioner (right preconditioning of GMRES):
+//   z_wall = -2 v_wall                         (the wall block's jump -1/2 I)
+//   t_b    = v_b - A_bw z_wall                 (wall -> body coupling, trapezoid)
+//   z_b    = B_b^{-1} t_b                      (exact per-body blocks, FP32)
+// B_b is the operator restricted to body b's density and its stokeslet and
+// rotlet unknowns (size m = 2n + 3, ordered sigma_x, sigma_y, l1, l2, xi).
+
+// Entries of B_b, FP32, row-major, one CTA per (body, row).
+__global__ void __launch_bounds__(256)
+k_pc_blocks(GeoDev G, float* __restrict__ B) {
+  const int b = blockIdx.x, row = blockIdx.y;
+  const int n = G.n, m = 2 * n + 3;
+  float* R = B + ((size_t)b * m + row) * m;
+  const int base = G.nout + b * n;
+  const double2 cb = G.cen[b];
+  if (row < 2 * n) {
+    const int i = row < n ? row : row - n;   // target node
+    const int comp = row < n ? 0 : 1;        // u or v
+    const int gi = base + i;
+    const double2 p = G.xy[gi];
+    for (int col = threadIdx.x; col < m; col += blockDim.x) {
+      double v = 0.0;
+      if (col < 2 * n) {
+        const int j = col < n ? col : col - n;
+        const int ccomp = col < n ? 0 : 1;
+        const int gj = base + j;
+        if (j != i) {
+          const double2 q = G.xy[gj], nn = G.nrm[gj];
+          const double rx = p.x - q.x, ry = p.y - q.y;
+          const double rho2 = rx * rx + ry * ry;
+          const double f = (rx * nn.x + ry * nn.y) * G.w[gj] / (rho2 * rho2);
+          v = f * (comp == 0 ? rx : ry) * (ccomp == 0 ? rx : ry);
+        } else {
+          const double2 nn = G.nrm[gi];
+          const double k = G.cur[gi] * G.sp[gi] / n;
+          if (comp == 0 && ccomp == 0) v = -k * nn.y * nn.y - 0.5;
+          else if (comp == 0 && ccomp == 1) v = k * nn.x * nn.y;
+          else if (comp == 1 && ccomp == 0) v = k * nn.y * nn.x;
+          else v = -k * nn.x * nn.x - 0.5;
+        }
+      } else {
+        const double rx = p.x - cb.x, ry = p.y - cb.y;
+        const double rho2 = rx * rx + ry * ry;
+        const double lg = log(rho2);
+        const int c = col - 2 * n;
+        const double q = 0.5 / EB_TWOPI;
+        if (c == 0) v = comp == 0 ? q * (-0.5 * lg + rx * rx / rho2) : q * (rx * ry / rho2);
+        else if (c == 1) v = comp == 0 ? q * (rx * ry / rho2) : q * (-0.5 * lg + ry * ry / rho2);
+        else v = comp == 0 ? ry / rho2 : -rx / rho2;
+      }
+      R[col] = (float)v;
+    }
+  } else {
+    const int c = row - 2 * n;
+    for (int col = threadIdx.x; col < m; col += blockDim.x) {
+      double v = 0.0;
+      if (col < 2 * n) {
+        const int j = col < n ? col : col - n;
+        const bool isx = col < n;
+        const int gj = base + j;
+        const double sp = G.sp[gj];
+        const double2 q = G.xy[gj];
+        if (c == 0) v = isx ? -sp / n : 0.0;
+        else if (c == 1) v = isx ? 0.0 : -sp / n;
+        else v = isx ? -q.y * sp / n : q.x * sp / n;
+      } else {
+        v = (col - 2 * n == c) ? 1.0 : 0.0;
+      }
+      R[col] = (float)v;
+    }
+  }
+}
+
+// In-place Gauss-Jordan inversion with partial pivoting of a batch of m x m
+// FP32 matrices, one CTA per matrix.  Singular pivots set *bad.
+__global__ void __launch_bounds__(1024)
+k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
+  extern __shared__ float gjs[];
+  float* prow = gjs;               // pivot row (m)
+  float* pcol = gjs + m;           // pivot column (m)
+  int* piv = (int*)(gjs + 2 * m);  // row swaps (m)
+  __shared__ float rv[32];
+  __shared__ int ri[32];
+  float* A = B + (size_t)blockIdx.x * m * m;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k = 0; k < m; ++k) {
+    // pivot search over rows k..m-1 of column k
+    float best = -1.f;
+    int bi = k;
+    for (int i = k + tid; i < m; i += nt) {
+      float a = fabsf(A[(size_t)i * m + k]);
+      if (a > best) { best = a; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+      int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
+    }
+    if ((tid & 31) == 0) { rv[tid >> 5] = best; ri[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid < 32) {
+      best = tid < (nt >> 5) ? rv[tid] : -1.f;
+      bi = tid < (nt >> 5) ? ri[tid] : k;
+      for (int o = 16; o > 0; o >>= 1) {
+        float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
+      }
+      if (tid == 0) { piv[k] = bi; if (!(best > 0.f)) atomicOr(bad, 1); }
+    }
+    __syncthreads();
+    const int p = piv[k];
+    if (p != k) {
+      for (int j = tid; j < m; j += nt) {
+        float t = A[(size_t)k * m + j];
+        A[(size_t)k * m + j] = A[(size_t)p * m + j];
+        A[(size_t)p * m + j] = t;
+      }
+      __syncthreads();
+    }
+    const float d = 1.f / A[(size_t)k * m + k];
+    for (int j = tid; j < m; j += nt) {
+      float v = (j == k) ? d : A[(size_t)k * m + j] * d;
+      A[(size_t)k * m + j] = v;
+      prow[j] = v;
+    }
+    for (int i = tid; i < m; i += nt) pcol[i] = (i == k) ? 0.f : A[(size_t)i * m + k];
+    __syncthreads();
+    // rows i != k: a_ij -= a_ik * prow_j (column k: a_ik = -a_ik * d)
+    for (int e = tid; e < m * m; e += nt) {
+      const int i = e / m, j = e - i * m;
+      if (i == k) continue;
+      const float f = pcol[i];
+      if (j == k) A[(size_t)i * m + j] = -f * d;
+      else A[(size_t)i * m + j] -= f * prow[j];
+    }
+    __syncthreads();
+  }
+  // undo the row swaps as column swaps, last first
+  for (int k = m - 1; k >= 0; --k) {
+    const int p = piv[k];
+    if (p != k) {
+      for (int i = tid; i < m; i += nt) {
+        float t = A[(size_t)i * m + k];
+        A[(size_t)i * m + k] = A[(size_t)i * m + p];
+        A[(size_t)i * m + p] = t;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// z_b = B_b^{-1} t_b for every body.  t is gathered from v (the body part of
+// the unknown vector) plus the wall coupling tw (per body node, FP64, already
+// the product A_bw z_wall); z is scattered into the same layout.  CTA = (body,
+// 256-row chunk), warp per row.
+__global__ void __launch_bounds__(256)
+k_pc_apply_bodies(GeoDev G, const float* __restrict__ Binv, const double* __restrict__ v,
+                  const double2* __restrict__ tw, double* __restrict__ z) {
+  extern __shared__ float tv[];   // m entries of t_b
+  const int b = blockIdx.x, n = G.n, m = 2 * n + 3;
+  const long long sb = 2LL * G.nout + 2LL * n * b;      // sigma block of body b
+  const long long cbk = 2LL * G.nout + 2LL * n * G.M + 3LL * b;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    double t;
+    if (r < n) t = v[sb + r] - tw[(size_t)b * n + r].x;
+    else if (r < 2 * n) t = v[sb + r] - tw[(size_t)b * n + (r - n)].y;
+    else t = v[cbk + (r - 2 * n)];
+    tv[r] = (float)t;
+  }
+  __syncthreads();
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = blockIdx.y * 8 + wid; r < m; r += gridDim.y * 8) {
+    const float* __restrict__ row = Binv + ((size_t)b * m + r) * m;
+    float acc = 0.f;
+    for (int c = lane; c < m; c += 32) acc = fmaf(__ldg(row + c), tv[c], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      if (r < 2 * n) z[sb + r] = (double)acc;
+      else z[cbk + (r - 2 * n)] = (double)acc;
+    }
+  }
+}
+
+// z_wall = -2 v_wall, and the FP32 source strengths w * z_wall of the wall
+// for the coupling sum.
+__global__ void k_pc_wall(GeoDev G, const double* __restrict__ v, double* __restrict__ z, float2* __restrict__ ws32) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.nout) return;
+  const double zx = -2.0 * v[g], zy = -2.0 * v[G.nout + g];
+  z[g] = zx;
+  z[G.nout + g] = zy;
+  const double w = G.w[g];
+  ws32[g] = make_float2((float)(w * zx), (float)(w * zy));
+}
+
+// A_bw z_wall: the wall's trapezoid double layer at every body node, FP32
+// with the same tile-relative coordinates as k_far32.  One thread per body
+// node; the wall tiles stream through shared memory.
+__global__ void __launch_bounds__(256)
+k_pc_wall2body(int nout, int nb, const float4* __restrict__ src, const float2* __restrict__ tgt,
+               const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+               const int4* __restrict__ tiles, int nwall_tiles, double2* __restrict__ out) {
+  __shared__ float4 sg[WALL_TS];
+  __shared__ float2 sw[WALL_TS];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < nb;
+  const int g = nout + (act ? i : nb - 1);
+  const float2 o = tgt[g];
+  const double2 a = anchor[g];
+  float hx = 0.f, lx = 0.f, hy = 0.f, ly = 0.f;
+  for (int ti = 0; ti < nwall_tiles; ++ti) {
+    const int4 T = tiles[ti];
+    __syncthreads();
+    if (threadIdx.x < T.y) { sg[threadIdx.x] = src[T.x + threadIdx.x]; sw[threadIdx.x] = ws32[T.x + threadIdx.x]; }
+    __syncthreads();
+    const double2 cs = tile_c[ti];
+    const float px = (float)(a.x - cs.x) + o.x, py = (float)(a.y - cs.y) + o.y;
+    float tx = 0.f, ty = 0.f;
+    for (int j = 0; j < T.y; ++j) {
+      const float4 s = sg[j];
+      const float2 w = sw[j];
+      float rx = px - s.x, ry = py - s.y;
+      float rho2 = fmaf(rx, rx, ry * ry);
+      float rdn = fmaf(rx, s.z, ry * s.w);
+      float rds = fmaf(rx, w.x, ry * w.y);
+      float inv = rcp_approx(rho2);
+      float c = (rdn * rds) * (inv * inv);
+      tx = fmaf(c, rx, tx);
+      ty = fmaf(c, ry, ty);
+    }
+    two_sum_add(hx, lx, tx);
+    two_sum_add(hy, ly, ty);
+  }
+  if (act) out[i] = make_double2((double)hx + (double)lx, (double)hy + (double)ly);
 }
 
 // ---------------------------------------------------------------------------
@@ -488,7 +898,7 @@ constexpr int SR_CHUNK = 256;
 __global__ void __launch_bounds__(256)
 k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ partial, int nsplit,
           const int* __restrict__ tptr, const int* __restrict__ tpairs, const double2* __restrict__ pair_out,
-          const double* __restrict__ sigdotn, double* __restrict__ vel) {
+          const double* __restrict__ sigdotn, const double2* __restrict__ selfp, double* __restrict__ vel) {
   __shared__ double4 sc[SR_CHUNK];   // cx, cy, stokeslet x, stokeslet y
   __shared__ double sr[SR_CHUNK];    // rotlet
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -498,6 +908,10 @@ k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ 
   double ux = 0.0, uy = 0.0;
   for (int q = 0; q < nsplit; ++q) {
     double2 v = partial[(size_t)q * G.N + gc];
+    ux += v.x; uy += v.y;
+  }
+  if (selfp) {
+    double2 v = selfp[gc];
     ux += v.x; uy += v.y;
   }
   if (tptr) {
@@ -641,6 +1055,12 @@ __global__ void k_scale(double* __restrict__ v, double a, long long n) {
 __global__ void k_bminus(const double* __restrict__ b, double* __restrict__ r, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) r[i] = b[i] - r[i];
+}
+
+// y += a x
+__global__ void k_axpy(double a, const double* __restrict__ x, double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a * x[i];
 }
 
 // out = a (copy) — used to seed the basis from a residual.

@@ -173,20 +173,44 @@ static void build_near(State& s, const std::vector<double2>& hxy, const std::vec
 static void build_tiles(State& s) {
   const Problem& pr = s.pr;
   std::vector<int4> tl;
-  auto add = [&](int start, int len, int c) {
-    for (int o = 0; o < len; o += FAR_TS) tl.push_back(make_int4(start + o, std::min(FAR_TS, len - o), c, 0));
+  auto add = [&](int start, int len, int c, int ts) {
+    for (int o = 0; o < len; o += ts) tl.push_back(make_int4(start + o, std::min(ts, len - o), c, 0));
   };
-  add(0, pr.nout, 0);
-  for (int b = 0; b < pr.M; ++b) add(pr.nout + b * pr.n, pr.n, 1 + b);
+  add(0, pr.nout, 0, WALL_TS);
+  s.nwall_tiles = (int)tl.size();
+  for (int b = 0; b < pr.M; ++b) add(pr.nout + b * pr.n, pr.n, 1 + b, FAR_TS);
   s.ntile = (int)tl.size();
-  int TB = (int)nblk(pr.N, FAR_NT * FAR_TPT);
-  int want = (int)std::ceil(8.0 * g_num_sms / TB);
-  s.nsplit = std::max(1, std::min(want, s.ntile));
-  std::vector<int> sp(s.nsplit + 1);
-  for (int q = 0; q <= s.nsplit; ++q) sp[q] = (int)((long long)q * s.ntile / s.nsplit);
+  auto splits = [&](int targets_per_cta, std::vector<int>& sp) {
+    int TB = (int)nblk(pr.N, targets_per_cta);
+    int want = (int)std::ceil(8.0 * g_num_sms / TB);
+    int ns = std::max(1, std::min(want, s.ntile));
+    sp.resize(ns + 1);
+    for (int q = 0; q <= ns; ++q) sp[q] = (int)((long long)q * s.ntile / ns);
+    return ns;
+  };
+  std::vector<int> sp64, sp32;
+  s.nsplit = splits(FAR_NT * FAR_TPT, sp64);
+  s.nsplit32 = splits(F32_NT * F32_TPT, sp32);
   h2d(s.tiles.ensure(tl.size()), tl.data(), tl.size(), s.st);
-  h2d(s.split_ptr.ensure(sp.size()), sp.data(), sp.size(), s.st);
-  s.partial.ensure((size_t)s.nsplit * pr.N);
+  h2d(s.split_ptr.ensure(sp64.size()), sp64.data(), sp64.size(), s.st);
+  h2d(s.split_ptr32.ensure(sp32.size()), sp32.data(), sp32.size(), s.st);
+  s.partial.ensure((size_t)std::max(s.nsplit, s.nsplit32) * pr.N);
+  // self-curve tasks: (first target, count <= 256, curve)
+  std::vector<int4> st;
+  for (int c = 0; c <= pr.M; ++c) {
+    int start = c == 0 ? 0 : pr.nout + (c - 1) * pr.n, len = c == 0 ? pr.nout : pr.n;
+    for (int o = 0; o < len; o += 256) st.push_back(make_int4(start + o, std::min(256, len - o), c, 0));
+  }
+  s.n_self_tasks = (int)st.size();
+  h2d(s.self_tasks.ensure(st.size()), st.data(), st.size(), s.st);
+  // pairs of distinct curves, less the near-masked ones (counted per launch)
+  long long same = (long long)pr.nout * (pr.nout - 1) + (long long)pr.M * pr.n * (pr.n - 1);
+  long long masked = 0;
+  for (int q = 0; q < s.near.nsrc; ++q) {
+    int c = s.near.h_src_curve[q];
+    masked += (long long)(s.near.h_src_ptr[q + 1] - s.near.h_src_ptr[q]) * (c == 0 ? pr.nout : pr.n);
+  }
+  s.far32_pairs = (long long)pr.N * (pr.N - 1) - same - masked;
   EB_CK(cudaStreamSynchronize(s.st));
 }
 
@@ -253,7 +277,56 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   }
   build_near(s, hxy, hsp, hcen, hrb);
   build_tiles(s);
+  s.src32.ensure(N);
+  s.ws32.ensure(N);
+  s.tgt32.ensure(N);
+  s.anchor.ensure(N);
+  s.selfsum.ensure(N);
+  s.tile_c.ensure(s.ntile);
+  k_geom32<<<s.ntile, 256, 0, st>>>(s.ntile, s.tiles.p, s.xy.p, s.nrm.p, s.tile_c.p, s.src32.p, s.tgt32.p,
+                                     s.anchor.p);
+  EB_LAUNCH_CHECK();
+  setup_preconditioner(s);
   s.geo_valid = true;
+}
+
+void setup_preconditioner(State& s) {
+  const Problem& pr = s.pr;
+  s.pc_active = false;
+  if (pr.P.precond != 1 || pr.M == 0) return;
+  const int n = pr.n, m = 2 * n + 3;
+  const GeoDev G = s.geo();
+  float* B = s.pcB.ensure((size_t)pr.M * m * m);
+  k_pc_blocks<<<dim3(pr.M, m), 256, 0, s.st>>>(G, B);
+  EB_LAUNCH_CHECK();
+  int* bad = s.pc_bad.ensure(1);
+  EB_CK(cudaMemsetAsync(bad, 0, sizeof(int), s.st));
+  const size_t smem = 3 * (size_t)m * sizeof(float);
+  if (smem > 48 * 1024) EB_CK(cudaFuncSetAttribute(k_gj_inv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
+  EB_LAUNCH_CHECK();
+  int hbad = 0;
+  d2h(&hbad, bad, 1, s.st);
+  EB_CK(cudaStreamSynchronize(s.st));
+  s.pc_z.ensure(pr.ntot);
+  s.pc_u.ensure(pr.ntot);
+  s.pc_tw.ensure((size_t)pr.M * n);
+  s.pc_ws32.ensure(pr.nout);
+  s.pc_active = hbad == 0;   // a singular block leaves the solve unpreconditioned
+}
+
+void apply_preconditioner(State& s, const double* v, double* z) {
+  const Problem& pr = s.pr;
+  const GeoDev G = s.geo();
+  const int n = pr.n, m = 2 * n + 3, nb = n * pr.M;
+  k_pc_wall<<<nblk(pr.nout, 256), 256, 0, s.st>>>(G, v, z, s.pc_ws32.p);
+  EB_LAUNCH_CHECK();
+  k_pc_wall2body<<<nblk(nb, 256), 256, 0, s.st>>>(pr.nout, nb, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
+                                                  s.pc_ws32.p, s.tiles.p, s.nwall_tiles, s.pc_tw.p);
+  EB_LAUNCH_CHECK();
+  dim3 g(pr.M, (unsigned)std::max(1, (m + 63) / 64));
+  k_pc_apply_bodies<<<g, 256, m * sizeof(float), s.st>>>(G, s.pcB.p, v, s.pc_tw.p, z);
+  EB_LAUNCH_CHECK();
 }
 
 void harvest_far_timing(State& s) {
@@ -261,11 +334,12 @@ void harvest_far_timing(State& s) {
   float ms = 0;
   EB_CK(cudaEventSynchronize(s.ef1));   // complete already on every path that calls this
   EB_CK(cudaEventElapsedTime(&ms, s.ef0, s.ef1));
-  s.stats.ms_far += ms;
+  if (s.far_kind == 1) s.stats.ms_far32 += ms;
+  else s.stats.ms_far += ms;
   s.far_pending = false;
 }
 
-void apply_operator(State& s, const double* d_den, double* d_vel) {
+void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
   harvest_far_timing(s);
   const Problem& pr = s.pr;
   const GeoDev G = s.geo();
@@ -273,14 +347,39 @@ void apply_operator(State& s, const double* d_den, double* d_vel) {
   cudaStream_t st = s.st;
   k_prep<<<pr.M + 1, 256, 0, st>>>(G, d_den, s.ws.p, d_vel, s.sigdotn.p);
   EB_LAUNCH_CHECK();
-  dim3 fg(nblk(pr.N, FAR_NT * FAR_TPT), s.nsplit);
-  EB_CK(cudaEventRecord(s.ef0, st));
-  if (nr.npairs > 0)
-    k_far64<true><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nr.mask.p, nr.mw, s.partial.p);
-  else
-    k_far64<false><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nullptr, 0, s.partial.p);
-  EB_LAUNCH_CHECK();
-  EB_CK(cudaEventRecord(s.ef1, st));
+  int nsplit;
+  if (prec == 1) {
+    k_ws32<<<nblk(pr.N, 256), 256, 0, st>>>(pr.N, s.ws.p, s.ws32.p);
+    EB_LAUNCH_CHECK();
+    dim3 fg(nblk(pr.N, F32_NT * F32_TPT), s.nsplit32);
+    EB_CK(cudaEventRecord(s.ef0, st));
+    if (nr.npairs > 0)
+      k_far32<true><<<fg, F32_NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
+                                           s.ws32.p, s.tiles.p, s.split_ptr32.p, nr.mask.p, nr.mw, s.partial.p);
+    else
+      k_far32<false><<<fg, F32_NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
+                                            s.ws32.p, s.tiles.p, s.split_ptr32.p, nullptr, 0, s.partial.p);
+    EB_LAUNCH_CHECK();
+    EB_CK(cudaEventRecord(s.ef1, st));
+    s.far_kind = 1;
+    k_self64<<<s.n_self_tasks, 256, 0, st>>>(G, s.ws.p, s.self_tasks.p, s.selfsum.p);
+    EB_LAUNCH_CHECK();
+    nsplit = s.nsplit32;
+    s.stats.matvecs_fp32++;
+    s.stats.far32_launches++;
+  } else {
+    dim3 fg(nblk(pr.N, FAR_NT * FAR_TPT), s.nsplit);
+    EB_CK(cudaEventRecord(s.ef0, st));
+    if (nr.npairs > 0)
+      k_far64<true><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nr.mask.p, nr.mw, s.partial.p);
+    else
+      k_far64<false><<<fg, FAR_NT, 0, st>>>(G, s.ws.p, s.tiles.p, s.split_ptr.p, nullptr, 0, s.partial.p);
+    EB_LAUNCH_CHECK();
+    EB_CK(cudaEventRecord(s.ef1, st));
+    s.far_kind = 0;
+    nsplit = s.nsplit;
+    s.stats.far_launches++;
+  }
   s.far_pending = true;
   if (nr.npairs > 0) {
     k_bdval<<<nr.n_bd_work, BD_NT, 0, st>>>(G, d_den, nr.bd_work.p, nr.src_curve.p, nr.bd_off.p, s.dker_wall.p,
@@ -290,11 +389,12 @@ void apply_operator(State& s, const double* d_den, double* d_vel) {
                                                     nr.pair_tgt.p, s.xy.p, s.pair_out.p);
     EB_LAUNCH_CHECK();
   }
-  k_combine<<<nblk(pr.N, 256), 256, 0, st>>>(G, d_den, s.partial.p, s.nsplit, nr.npairs ? nr.tptr.p : nullptr,
-                                             nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p, d_vel);
+  k_combine<<<nblk(pr.N, 256), 256, 0, st>>>(G, d_den, s.partial.p, nsplit, nr.npairs ? nr.tptr.p : nullptr,
+                                             nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p,
+                                             prec == 1 ? s.selfsum.p : nullptr, d_vel);
   EB_LAUNCH_CHECK();
   s.stats.matvecs++;
-  s.stats.far_launches++;
+  s.stats.far32_pairs = s.far32_pairs;
 }
 
 void build_rhs(State& s, double* d_rhs) {
@@ -345,8 +445,16 @@ static double* pinned(State& s, size_t n) {
   return s.h_pinned;
 }
 
-int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl_in, double tol,
-                long long* iters, double* est) {
+// One GMRES run with the semantics of SLATEC DGMRES as solveBIE calls it
+// (stokesSolver.f:481-497, gmres_routines.f): no restart, MAXL = min(maxl, N),
+// stop when the Givens estimate rho <= abs_tol, least squares by DHELS, x += V y.
+// The Arnoldi step is classical Gram-Schmidt applied twice (two passes of
+// tall-skinny products instead of DORTH's k sequential dot/axpy pairs).
+// d_r holds the initial residual on entry.  Operator precision: FP64, or, when
+// relax_abs > 0, FP32 far field once rho < relax_abs (inexact Krylov: the
+// operator error tolerated grows as the residual shrinks).
+static int gmres_cycle(State& s, double* d_r, double* d_x, long long maxl_in, double abs_tol, double relax_abs,
+                       long long* iters, double* rho_out) {
   const long long N = s.pr.ntot;
   const long long ldv = (N + 31) & ~31LL;
   long long MAXL = maxl_in;
@@ -354,45 +462,26 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   if (MAXL > N) MAXL = N;
   *iters = 0;
   cudaStream_t st = s.st;
-  const double bnrm = device_norm(s, d_b, N);
-  double* r = s.d_r.ensure(N);
-  if (x0_zero) {
-    k_copy<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
-    EB_LAUNCH_CHECK();
-  } else {
-    apply_operator(s, d_x, r);
-    k_bminus<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
-    EB_LAUNCH_CHECK();
-  }
   long long cap0 = std::min<long long>(MAXL + 1, 64);
-  if (s.vcap < cap0 || (long long)s.V.cap < cap0 * ldv) {
-    s.V.ensure((size_t)cap0 * ldv);
-    s.vcap = cap0;
-  } else {
-    s.vcap = (long long)(s.V.cap / ldv);
-  }
-  k_copy<<<nblk(N, 256), 256, 0, st>>>(r, s.V.p, N);
+  if ((long long)(s.V.cap / ldv) < cap0) s.V.ensure((size_t)cap0 * ldv);
+  s.vcap = (long long)(s.V.cap / ldv);
+  s.zcap = (long long)(s.Z.cap / ldv);
+  k_copy<<<nblk(N, 256), 256, 0, st>>>(d_r, s.V.p, N);
   EB_LAUNCH_CHECK();
   const double r0nrm = device_norm(s, s.V.p, N);
-  if (bnrm == 0.0) {
-    EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
-    EB_CK(cudaStreamSynchronize(st));
-    *est = 0.0;
-    throw Error(EROSION_BAD_INPUT, "zero right-hand side: the zero density was returned");
-  }
-  *est = r0nrm / bnrm;
+  *rho_out = r0nrm;
   if (!std::isfinite(r0nrm)) throw Error(EROSION_BREAKDOWN, "non-finite initial residual");
-  if (*est <= tol) return EROSION_OK;
+  if (r0nrm <= abs_tol) return EROSION_OK;
   k_scale<<<nblk(N, 256), 256, 0, st>>>(s.V.p, 1.0 / r0nrm, N);
   EB_LAUNCH_CHECK();
-
   std::vector<std::vector<double>> HES;   // column ll-1 holds HES(1..ll+1, ll)
   std::vector<double> Q;
   double prod = 1.0, rho = r0nrm;
   long long lgmr = 0;
   int iflag = -1;
   double* hdev = s.hdev.ensure((size_t)MAXL + 2);
-  double* hp = pinned(s, (size_t)MAXL + 2);
+  double* hs = s.ydev.ensure((size_t)MAXL + 2);
+  double* hp = pinned(s, 2 * (size_t)MAXL + 4);
   for (long long ll = 1; ll <= MAXL; ++ll) {
     lgmr = ll;
     if (ll + 1 > s.vcap) {
@@ -402,25 +491,37 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
     }
     double* V = s.V.p;
     double* vnew = V + ll * ldv;
-    apply_operator(s, V + (ll - 1) * ldv, vnew);
-    // Classical Gram-Schmidt, applied twice.
+    const int prec = (relax_abs > 0.0 && rho < relax_abs) ? 1 : 0;
+    if (s.pc_active) {
+      // flexible GMRES: keep z_k = P^{-1} v_k so that x = x0 + Z y is exactly
+      // consistent with the Arnoldi relation A Z = V H whatever the
+      // preconditioner's rounding
+      if (ll > s.zcap) {
+        long long nc = std::min<long long>(MAXL, std::max<long long>(2 * s.zcap, std::max<long long>(ll, 64)));
+        s.Z.grow_keep((size_t)nc * ldv, (size_t)(ll - 1) * ldv, st);
+        s.zcap = nc;
+      }
+      double* zk = s.Z.p + (ll - 1) * ldv;
+      apply_preconditioner(s, V + (ll - 1) * ldv, zk);
+      apply_operator(s, zk, vnew, prec);
+    } else {
+      apply_operator(s, V + (ll - 1) * ldv, vnew, prec);
+    }
     const int k = (int)ll;
     dots(s, V, ldv, k, vnew, N, hdev, 0);
     k_vh<<<nblk(N, 256), 256, 0, st>>>(V, ldv, k, hdev, -1.0, vnew, N);
     EB_LAUNCH_CHECK();
-    double* hs = s.ydev.ensure((size_t)MAXL + 2);   // second-pass coefficients
     dots(s, V, ldv, k, vnew, N, hs, 0);
     k_vh<<<nblk(N, 256), 256, 0, st>>>(V, ldv, k, hs, -1.0, vnew, N);
     EB_LAUNCH_CHECK();
     dots(s, vnew, N, 1, vnew, N, hdev + k, 0);
     d2h(hp, hdev, (size_t)k + 1, st);
-    std::vector<double> h2h(k);
-    d2h(h2h.data(), hs, (size_t)k, st);
+    d2h(hp + MAXL + 2, hs, (size_t)k, st);
     EB_CK(cudaStreamSynchronize(st));
     harvest_far_timing(s);
     const double snormw = std::sqrt(hp[k]);
     std::vector<double> col(ll + 1);
-    for (int i = 0; i < k; ++i) col[i] = hp[i] + h2h[i];
+    for (int i = 0; i < k; ++i) col[i] = hp[i] + hp[MAXL + 2 + i];
     col[ll] = snormw;
     bool finite = std::isfinite(snormw);
     for (int i = 0; i < k && finite; ++i) finite = std::isfinite(col[i]);
@@ -442,13 +543,13 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
     if (col[ll - 1] == 0.0) { iflag = 2; break; }
     prod = prod * sn;
     rho = std::fabs(prod * r0nrm);
-    *est = rho / bnrm;
-    if (*est <= tol) { iflag = 0; break; }
+    if (rho <= abs_tol) { iflag = 0; break; }
     if (ll == MAXL) { iflag = (rho < r0nrm) ? 1 : 2; break; }
     k_scale<<<nblk(N, 256), 256, 0, st>>>(vnew, 1.0 / snormw, N);
     EB_LAUNCH_CHECK();
   }
   *iters = lgmr;
+  *rho_out = rho;
   if (iflag == 3) throw Error(EROSION_BREAKDOWN, "non-finite value in the Arnoldi process");
   if (iflag == 2) return EROSION_BREAKDOWN;
   // DHELS (gmres_routines.f:1048) and x += V y.
@@ -469,10 +570,77 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   }
   double* yd = s.ydev.ensure((size_t)L + 1);
   h2d(yd, y.data(), (size_t)L, st);
-  k_vh<<<nblk(N, 256), 256, 0, st>>>(s.V.p, ldv, (int)L, yd, 1.0, d_x, N);
-  EB_LAUNCH_CHECK();
+  if (s.pc_active) {   // x += Z y
+    k_vh<<<nblk(N, 256), 256, 0, st>>>(s.Z.p, ldv, (int)L, yd, 1.0, d_x, N);
+    EB_LAUNCH_CHECK();
+  } else {
+    k_vh<<<nblk(N, 256), 256, 0, st>>>(s.V.p, ldv, (int)L, yd, 1.0, d_x, N);
+    EB_LAUNCH_CHECK();
+  }
   EB_CK(cudaStreamSynchronize(st));
   return iflag == 1 ? EROSION_MAXITER : EROSION_OK;
+}
+
+// Default switch point of the mixed-precision operator: FP32 far field once
+// the GMRES residual estimate is below kRelaxFactor * tol.  The FP32 far field
+// has a relative operator error of ~1e-9; switching much earlier leaves a gap
+// between the estimated and the true residual that costs FP64 refinement
+// restarts (measured on the 100-body workload: 1e-3 -> 7 sweeps, 1e-6 -> 1).
+static const double kRelaxFactor = 100.0;
+
+int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
+                long long* iters, double* est) {
+  const long long N = s.pr.ntot;
+  cudaStream_t st = s.st;
+  *iters = 0;
+  const double bnrm = device_norm(s, d_b, N);
+  if (bnrm == 0.0) {
+    EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
+    EB_CK(cudaStreamSynchronize(st));
+    *est = 0.0;
+    throw Error(EROSION_BAD_INPUT, "zero right-hand side: the zero density was returned");
+  }
+  double* r = s.d_r.ensure(N);
+  auto residual = [&](bool zero) {   // r = b - A x with the FP64 operator
+    if (zero) {
+      k_copy<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
+      EB_LAUNCH_CHECK();
+    } else {
+      apply_operator(s, d_x, r, 0);
+      k_bminus<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
+      EB_LAUNCH_CHECK();
+    }
+  };
+  residual(x0_zero);
+  if (s.pr.P.precision == 0) {
+    long long it = 0;
+    double rho = 0;
+    int rc = gmres_cycle(s, r, d_x, maxl, tol * bnrm, 0.0, &it, &rho);
+    *iters = it;
+    *est = rho / bnrm;
+    return rc;
+  }
+  // Mixed precision: relaxed FP32 cycles inside FP64 iterative refinement.
+  long long total = 0;
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    long long it = 0;
+    double rho = 0;
+    const double relax = s.pr.P.relax_tol > 0 ? s.pr.P.relax_tol : tol * kRelaxFactor;
+    int rc = gmres_cycle(s, r, d_x, std::max<long long>(maxl - total, 1), tol * bnrm, relax * bnrm, &it, &rho);
+    total += it;
+    s.stats.sweeps = sweep + 1;
+    if (rc == EROSION_BREAKDOWN) { *iters = total; *est = rho / bnrm; return rc; }
+    residual(false);
+    const double tr = device_norm(s, r, N) / bnrm;
+    s.stats.true_residual = tr;
+    s.stats.true_residual_checks += 1;
+    *est = tr;
+    if (!std::isfinite(tr)) throw Error(EROSION_BREAKDOWN, "non-finite true residual");
+    if (tr <= tol) { *iters = total; return EROSION_OK; }
+    if (total >= maxl) { *iters = total; return EROSION_MAXITER; }
+  }
+  *iters = total;
+  return EROSION_MAXITER;
 }
 
 }  // namespace eb
@@ -535,7 +703,7 @@ int solve_device_impl(State& s, double* d_den, bool x0_zero, int64_t* nits) {
   double est = 0;
   int rc = gmres_solve(s, rhs, d_den, x0_zero, pr.P.maxl, pr.P.tol, &it, &est);
   s.stats.iterations = it;
-  s.stats.sweeps = 1;
+  if (s.stats.sweeps == 0) s.stats.sweeps = 1;
   s.stats.est_residual = est;
   s.stats.near_pairs = s.near.npairs;
   if (pr.P.true_residual) {
@@ -637,7 +805,7 @@ int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t
     double* dd = s.d_den.ensure(ntot);
     double* dv = s.d_w.ensure(ntot);
     h2d(dd, density, ntot, s.st);
-    apply_operator(s, dd, dv);
+    apply_operator(s, dd, dv, s.pr.P.precision == 1 ? 1 : 0);
     d2h(vel, dv, ntot, s.st);
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
@@ -724,7 +892,8 @@ void erosion_release(void) {
   State& s = state();
   std::lock_guard<std::mutex> lk(s.mu);
   DBuf<double>* dbs[] = {&s.dker_body, &s.dker_wall, &s.wx, &s.wy, &s.sp, &s.cur, &s.w, &s.rb, &s.sigdotn,
-                         &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.part, &s.hdev, &s.ydev};
+                         &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.Z, &s.part, &s.hdev,
+                         &s.ydev, &s.pc_z, &s.pc_u};
   for (auto* b : dbs) b->release();
   DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.partial, &s.bd, &s.pair_out};
   for (auto* b : d2s) b->release();
@@ -732,6 +901,10 @@ void erosion_release(void) {
   s.near.bd_off.release(); s.near.bd_work.release(); s.near.bary_work.release(); s.near.mask.release();
   s.tiles.release(); s.split_ptr.release();
   s.vcap = 0;
+  s.zcap = 0;
+  s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
+  s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
+  s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release();
   s.dker_body_n = s.dker_wall_n = -1;
   s.geo_valid = false;
 }

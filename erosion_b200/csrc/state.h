@@ -125,8 +125,25 @@ struct State {
 
   // far field
   DBuf<int4> tiles;
-  DBuf<int> split_ptr;
-  int nsplit = 0, ntile = 0;
+  DBuf<int> split_ptr, split_ptr32;
+  int nsplit = 0, nsplit32 = 0, ntile = 0;
+  // mixed precision: FP32 geometry, strengths, self-curve tasks and sums
+  DBuf<float4> src32;
+  DBuf<float2> ws32, tgt32;
+  DBuf<double2> tile_c, anchor;
+  DBuf<int4> self_tasks;
+  int n_self_tasks = 0;
+  DBuf<double2> selfsum;
+  long long far32_pairs = 0;
+  // block Gauss-Seidel preconditioner
+  bool pc_active = false;
+  int nwall_tiles = 0;
+  DBuf<float> pcB;          // M inverse blocks of (2n+3)^2
+  DBuf<double> pc_z, pc_u;  // scratch vectors
+  DBuf<double2> pc_tw;      // A_bw z_wall per body node
+  DBuf<float2> pc_ws32;     // wall strengths of the coupling sum
+  DBuf<int> pc_bad;
+  int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32
 
   // work buffers
   DBuf<double2> ws, partial, bd, pair_out;
@@ -134,8 +151,9 @@ struct State {
   DBuf<double> d_xx, d_yy, d_den, d_rhs, d_r, d_w;
 
   // Krylov
-  DBuf<double> V, part, hdev, ydev;
+  DBuf<double> V, Z, part, hdev, ydev;
   long long vcap = 0;   // vectors held by V
+  long long zcap = 0;   // vectors held by Z (preconditioned basis, flexible GMRES)
   double* h_pinned = nullptr;
   size_t h_pinned_cap = 0;
 
@@ -156,12 +174,17 @@ void ensure_init(State& s);
 
 // Geometry + near lists + far-field tiles for (xx, yy) already on the device.
 void setup_problem(State& s, const Problem& pr, const double* d_xx, const double* d_yy);
-// vel = A den (FP64 operator), device pointers.
-void apply_operator(State& s, const double* d_den, double* d_vel);
+// vel = A den, device pointers.  prec 0: FP64 far field; 1: FP32 far field
+// between distinct curves + FP64 self-curve sums.
+void apply_operator(State& s, const double* d_den, double* d_vel, int prec = 0);
 void build_rhs(State& s, double* d_rhs);
 // GMRES (SLATEC DGMRES semantics, CGS2 Arnoldi); returns EROSION_* status.
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
                 long long* iters, double* est);
+// Builds (or disables) the block preconditioner for the current geometry.
+void setup_preconditioner(State& s);
+// z = P^{-1} v (device vectors of length ntot).
+void apply_preconditioner(State& s, const double* v, double* z);
 double device_norm(State& s, const double* d_v, long long n);
 // Adds the last far-field launch's event time to stats.ms_far (after a sync).
 void harvest_far_timing(State& s);

@@ -96,7 +96,15 @@ typedef struct {
                            stokeslet (1,2) + rotlet 3 at the origin (:220-257);
                            2 homogeneous (all-zero) data                           */
   int32_t true_residual;/* 1: also evaluate ||b - A x||/||b|| with the FP64 operator */
-  int32_t reserved[6];
+  int32_t precond;      /* 0: none (the reference: JPRE = 0, stokesSolver.f:490);
+                           1: block Gauss-Seidel right preconditioner - wall block
+                           -2 I, wall-to-body coupling, exact inverse of every
+                           body's (2 npts + 3) block in FP32.  The stopping test is
+                           unchanged: ||b - A x||/||b|| <= tol                      */
+  int32_t reserved[5];
+  double relax_tol;     /* mixed mode: GMRES switches to the FP32 far field once its
+                           residual estimate is below relax_tol (relative);
+                           0 selects the library default                           */
 } erosion_params;
 
 /* Fills the reference's defaults: wall (3, 1, 8), tol 1e-8, maxl 8000, ibary 1,
@@ -112,9 +120,13 @@ typedef struct {
   double est_residual;      /* GMRES estimate rho/||b|| at exit                    */
   double true_residual;     /* ||b - A x||/||b|| (FP64 operator) when requested    */
   double ms_total;          /* device time of the solve                            */
-  double ms_far;            /* device time inside the far-field kernel             */
-  int64_t far_launches;     /* far-field kernel launches                           */
+  double ms_far;            /* device time inside the FP64 far-field kernel        */
+  int64_t far_launches;     /* FP64 far-field kernel launches                      */
   int64_t near_pairs;       /* (target node, source curve) barycentric pairs       */
+  double ms_far32;          /* device time inside the FP32 far-field kernel        */
+  int64_t far32_launches;   /* FP32 far-field kernel launches                      */
+  int64_t far32_pairs;      /* source-target pairs per FP32 far-field launch       */
+  double true_residual_checks; /* FP64 true-residual evaluations (mixed mode)      */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
@@ -128,7 +140,9 @@ int erosion_solve_device(const erosion_params* p, int64_t npts, int64_t nbods, i
 void erosion_get_solve_stats(erosion_solve_stats* s);
 
 /* One application of the boundary operator (host arrays) — the reference's
- * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm. */
+ * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm;
+ * precision = 1 applies the mixed-precision operator (FP32 far field between
+ * distinct curves, FP64 elsewhere). */
 int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                    const double* xx, const double* yy, const double* density, double* vel);
 

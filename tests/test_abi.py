@@ -38,8 +38,8 @@ def test_binding_covers_header():
 
 
 def test_param_struct_layout():
-    # erosion_params: 4 doubles, int64, 6 int32 flags, 6 reserved int32
-    assert ctypes.sizeof(_lib.ErosionParams) == 4 * 8 + 8 + 6 * 4 + 6 * 4
+    # erosion_params: 4 doubles, int64, 6 int32 flags, 6 reserved int32, 1 double
+    assert ctypes.sizeof(_lib.ErosionParams) == 4 * 8 + 8 + 6 * 4 + 6 * 4 + 8
     p = _lib.default_params()
     assert (p.wall_a, p.wall_b, p.wall_order, p.tol, p.maxl) == (3.0, 1.0, 8.0, 1e-8, 8000)
     assert (p.ibary, p.ifmm, p.ibc, p.precision) == (1, 1, 1, 0)
