@@ -59,8 +59,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--precision", type=int, default=1, help="0 FP64, 1 mixed (FP32 far field + FP64 refinement)")
+    ap.add_argument("--precond", type=int, default=1, help="0 none (reference), 1 block Gauss-Seidel")
     ap.add_argument("--warm-start", type=int, default=0)
+    ap.add_argument("--compare-plain", type=int, default=1,
+                    help="also time one step of the plain FP64 unpreconditioned form")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -236,7 +239,8 @@ def main():
     g = G.workload(args.workload, seed=args.seed + rank)
     th, ln, xs, ys = G.to_thetalen(g)
     M0, n = g.M, g.n
-    p = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=args.precision)
+    p = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=args.precision, precond=args.precond)
+    p_plain = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=0, precond=0)
     sp = _lib.StepParams()
     L.erosion_default_step_params(ctypes.byref(sp), n)
     sp.dt = wl["dt"]
@@ -254,8 +258,9 @@ def main():
     deleted = np.zeros(M0, np.int64)
     PI64, PD = _lib.PI64, _lib.PD
 
-    def step():
-        rc = L.erosion_rk2_step_device(ctypes.byref(p), ctypes.byref(sp), n, nb.ctypes.data_as(PI64), g.nout,
+    def step(params=None):
+        params = params or p
+        rc = L.erosion_rk2_step_device(ctypes.byref(params), ctypes.byref(sp), n, nb.ctypes.data_as(PI64), g.nout,
                                        d_th.data_ptr(), d_ln.data_ptr(), d_xs.data_ptr(), d_ys.data_ptr(),
                                        tt.ctypes.data_as(PD), deleted.ctypes.data_as(PI64))
         _lib.check(rc, (_lib.EROSION_OK, _lib.EROSION_MAXITER))
@@ -299,25 +304,41 @@ def main():
         ms = float(t.item())
     value = world * args.steps / (ms * 1e-3)
 
-    # roofline of the far-field kernel (FP64 pipe)
-    far_ms = s1["ms_far"] - s0["ms_far"]
-    far_n = s1["far_launches"] - s0["far_launches"]
+    # roofline of the dominant far-field kernel: FP64 (k_far64) or FP32
+    # (k_far32), against the measured FMA peak of the pipe it runs on
     N = g.nout + n * int(nb[0])
-    flops_launch = 20.0 * N * (N - 1)
-    avg_ms = far_ms / max(far_n, 1)
-    achieved = flops_launch / (avg_ms * 1e-3) / 1e12
+    far64_ms = s1["ms_far"] - s0["ms_far"]
+    far64_n = s1["far_launches"] - s0["far_launches"]
+    far32_ms = s1["ms_far32"] - s0["ms_far32"]
+    far32_n = s1["far32_launches"] - s0["far32_launches"]
     peak64 = L.erosion_peak_tflops(0)
+    peak32 = L.erosion_peak_tflops(1)
+    kernels = {}
+    if far64_n:
+        a = 20.0 * s1["far32_pairs"] / (far64_ms / far64_n * 1e-3) / 1e12
+        kernels["k_far64"] = {"launches": far64_n, "ms_total": far64_ms, "ms_avg": far64_ms / far64_n,
+                              "pairs_per_launch": s1["far32_pairs"], "achieved_tflops": a, "peak_tflops": peak64,
+                              "frac": a / peak64, "share_of_timed": far64_ms / ms}
+    if far32_n:
+        pairs32 = s1["far32_pairs"]
+        a = 20.0 * pairs32 / (far32_ms / far32_n * 1e-3) / 1e12
+        kernels["k_far32"] = {"launches": far32_n, "ms_total": far32_ms, "ms_avg": far32_ms / far32_n,
+                              "pairs_per_launch": pairs32, "achieved_tflops": a, "peak_tflops": peak32,
+                              "frac": a / peak32, "share_of_timed": far32_ms / ms}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"]) if kernels else None
     traffic = None
     try:
         with open(TRAFFIC_FILE) as f:
-            traffic = json.load(f).get(args.workload)
+            traffic = json.load(f).get(f"{args.workload}:{dom}") or json.load(open(TRAFFIC_FILE)).get(args.workload)
     except Exception:
         pass
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                "frac": achieved / peak64 if peak64 > 0 else None, "traffic": traffic,
-                "kernel": "k_far64", "algorithmic": "20 flops x N(N-1) source-target pairs per launch",
-                "peak_source": "measured FP64 FMA loop on this GPU (erosion_peak_tflops)",
-                "far_ms_avg": avg_ms, "far_share_of_step": far_ms / ms if ms > 0 else None}
+    roofline = {"bound": "fp64" if dom == "k_far64" else "fp32", "achieved": kernels[dom]["achieved_tflops"] if dom else None,
+                "peak": kernels[dom]["peak_tflops"] if dom else None, "unit": "TFLOP/s",
+                "frac": kernels[dom]["frac"] if dom else None, "traffic": traffic, "kernel": dom,
+                "algorithmic": "20 flops per source-target pair; pairs per launch = node pairs of distinct curves "
+                               "less the barycentric near pairs (self-curve pairs run in k_self64)",
+                "peak_source": "measured FMA loop on this GPU (erosion_peak_tflops), vector pipe",
+                "kernels": kernels}
 
     # end to end through the host-array entry point (state in host memory)
     e2e = None
@@ -353,10 +374,27 @@ def main():
                "entry_point": "erosion_rk2_step (host arrays)"}
 
     mean_iters = float(np.mean(iters)) if iters else 0.0
+    plain = None
+    if args.compare_plain:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0.record(stream)
+            stp = step(p_plain)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        plain = {"value": 1.0 / (pms * 1e-3) * world, "unit": "steps/s", "steps": 1,
+                 "gmres_iterations_per_step": sum(stp["gmres_iterations"]),
+                 "form": "FP64 operator, no preconditioner, zero initial guess (the reference's algorithm)",
+                 "speedup_of_value": value / (1.0 / (pms * 1e-3) * world)}
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            v, nth, sample, t_step = cpu_rate(g, mean_iters, args.cpu_seconds)
+            it_ref = plain["gmres_iterations_per_step"] if plain else (load_iterations(args.workload) or {}).get(
+                "iterations_per_step", mean_iters)
+            v, nth, sample, t_step = cpu_rate(g, it_ref, args.cpu_seconds)
             cpu = {"value": v, "unit": "steps/s", "cores": nth, "kind": "port", "sample": sample}
         pairs_per_s = (s1["matvecs"] - s0["matvecs"]) * N * (N - 1) / (ms * 1e-3) * world
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
@@ -368,6 +406,7 @@ def main():
                           "dt_note": f"configured dt {wl['dt_config']} deletes every body in step 1 at this "
                                      f"shear-stress scale; scaled to keep the bodies", "fixpdrop": 0, "tol": 1e-8,
                           "precision": "fp64" if args.precision == 0 else "mixed", "warm_start": args.warm_start,
+                          "precond": "block Gauss-Seidel" if args.precond else "none",
                           "parallelism": "replicas" if world > 1 else "single GPU",
                           "l2": "flushed (256 MiB write) before every step"},
                "gmres_iterations_per_step": mean_iters,
@@ -375,6 +414,7 @@ def main():
                "gmres_solves_per_s": 2 * value,
                "step_breakdown_ms": {k: float(np.mean([s[k] for s in per_step])) for k in
                                      ("ms_solve", "ms_stress", "ms_thetalen", "ms_total")},
+               "plain_fp64": plain,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk.summary()}
         print(json.dumps(out), flush=True)

@@ -75,10 +75,16 @@ class SolveStats(ctypes.Structure):
         ("far32_launches", c_int64),
         ("far32_pairs", c_int64),
         ("true_residual_checks", c_double),
+        ("sweep_residual", c_double * 8),
+        ("sweep_iterations", c_int64 * 8),
+        ("floor_accepted", c_int64),
     ]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["sweep_residual"] = list(self.sweep_residual)[: max(self.sweeps, 0)]
+        d["sweep_iterations"] = list(self.sweep_iterations)[: max(self.sweeps, 0)]
+        return d
 
 
 class StepParams(ctypes.Structure):

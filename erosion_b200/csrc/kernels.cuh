@@ -103,51 +103,104 @@ __global__ void k_body_stats(int n, int nout, const double2* __restrict__ xy, co
 }
 
 // ---------------------------------------------------------------------------
-// Per-matvec preparation: one CTA per curve.  Writes the weighted source
-// strengths w*sigma used by the far field, the constraint rows of every body
-// (:1055-1096) and the wall's integral of sigma.n for the rank-one term
-// (:1107-1111).
+// Per-matvec preparation: one CTA per curve.  Writes
+//   ws    = w * sigma               (full strengths: self-curve sums)
+//   wrest = w * (sigma - rigid part) (strengths seen by other curves)
+// the constraint rows of every body (:1055-1096) and the wall's integral of
+// sigma.n for the rank-one term (:1107-1111).  The rigid part of a body's
+// density is its speed-weighted projection on the translations and the
+// rotation about the speed-weighted centroid: a rigid-motion density has a
+// zero double layer outside its curve, so removing it changes the far field
+// only at the rounding level while the sums stop cancelling terms of size
+// |sigma_rigid| (large for small bodies: the stokeslet/rotlet completion puts
+// ~lambda/r and ~xi/r^3 into these modes).  The split is made only when the
+// close pairs are masked for the barycentric correction (split_rigid = 1): at a
+// few node spacings the trapezoid rule's error on a rigid mode is ~1e-9.
 __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict__ den,
-                                              double2* __restrict__ ws, double* __restrict__ vel,
-                                              double* __restrict__ sigdotn) {
+                                              double2* __restrict__ ws, double2* __restrict__ wrest,
+                                              float2* __restrict__ ws32, double* __restrict__ vel,
+                                              double* __restrict__ sigdotn, int split_rigid) {
   __shared__ double sh[32];
   const int c = blockIdx.x;
   const int start = curve_start(G, c), len = curve_len(G, c);
-  double a0 = 0, a1 = 0, a2 = 0;
-  for (int j = threadIdx.x; j < len; j += blockDim.x) {
-    int g = start + j;
-    double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
-    double wg = G.w[g], s = G.sp[g];
-    ws[g] = make_double2(wg * sx, wg * sy);
-    if (c == 0) {
-      double2 nn = G.nrm[g];
-      a0 += (nn.x * sx + nn.y * sy) * s;
-    } else {
-      double2 p = G.xy[g];
-      a0 += sx * s;
-      a1 += sy * s;
-      a2 += (sx * p.y - sy * p.x) * s;
-    }
-  }
-  a0 = block_sum<256>(a0, sh);
   if (c == 0) {
+    double a0 = 0;
+    for (int j = threadIdx.x; j < len; j += blockDim.x) {
+      int g = start + j;
+      double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+      double wg = G.w[g];
+      double2 v = make_double2(wg * sx, wg * sy);
+      ws[g] = v;
+      wrest[g] = v;
+      ws32[g] = make_float2((float)v.x, (float)v.y);
+      double2 nn = G.nrm[g];
+      a0 += (nn.x * sx + nn.y * sy) * G.sp[g];
+    }
+    a0 = block_sum<256>(a0, sh);
     if (threadIdx.x == 0) *sigdotn = a0 * (EB_TWOPI / len);
     return;
   }
+  // pass 1: constraint sums and the weighted means
+  double a0 = 0, a1 = 0, a2 = 0, s0 = 0, sxw = 0, syw = 0;
+  for (int j = threadIdx.x; j < len; j += blockDim.x) {
+    int g = start + j;
+    double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+    double s = G.sp[g];
+    double2 p = G.xy[g];
+    a0 += sx * s;
+    a1 += sy * s;
+    a2 += (sx * p.y - sy * p.x) * s;
+    s0 += s;
+    sxw += s * p.x;
+    syw += s * p.y;
+  }
+  a0 = block_sum<256>(a0, sh);
   a1 = block_sum<256>(a1, sh);
   a2 = block_sum<256>(a2, sh);
+  s0 = block_sum<256>(s0, sh);
+  sxw = block_sum<256>(sxw, sh);
+  syw = block_sum<256>(syw, sh);
   if (threadIdx.x == 0) {
     int b = c - 1;
     vel[ic_of(G, b, 0)] = (-a0) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 0)];
     vel[ic_of(G, b, 1)] = (-a1) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 1)];
     vel[ic_of(G, b, 2)] = (-a2) / EB_TWOPI * (EB_TWOPI / len) + den[ic_of(G, b, 2)];
   }
+  const double xb = sxw / s0, yb = syw / s0;
+  // pass 2: rotation coefficient about (xb, yb); phi3 = (-(y - yb), x - xb)
+  double r0 = 0, r1 = 0;
+  for (int j = threadIdx.x; j < len; j += blockDim.x) {
+    int g = start + j;
+    double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+    double s = G.sp[g];
+    double2 p = G.xy[g];
+    double fx = -(p.y - yb), fy = p.x - xb;
+    r0 += s * (fx * sx + fy * sy);
+    r1 += s * (fx * fx + fy * fy);
+  }
+  r0 = block_sum<256>(r0, sh);
+  r1 = block_sum<256>(r1, sh);
+  double t1 = a0 / s0, t2 = a1 / s0, t3 = r1 > 0 ? r0 / r1 : 0.0;
+  if (!split_rigid) t1 = t2 = t3 = 0.0;
+  for (int j = threadIdx.x; j < len; j += blockDim.x) {
+    int g = start + j;
+    double sx = den[ix_of(G, g)], sy = den[iy_of(G, g)];
+    double2 p = G.xy[g];
+    double wg = G.w[g];
+    ws[g] = make_double2(wg * sx, wg * sy);
+    double rx = sx - t1 + t3 * (p.y - yb), ry = sy - t2 - t3 * (p.x - xb);
+    double2 v = make_double2(wg * rx, wg * ry);
+    wrest[g] = v;
+    ws32[g] = make_float2((float)v.x, (float)v.y);
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Far field, FP64: u_i = sum_{j != i} (r.n_j)(r.w_j sigma_j)/rho^4 r,
-// r = x_i - x_j, over every node pair except the (target, source curve) pairs
-// that the near-field bookkeeping replaces (bit c of mask[i]).  This is the
+// r = x_i - x_j, over every pair of distinct curves except the (target,
+// source curve) pairs that the near-field bookkeeping replaces (bit c of
+// mask[i]); pairs within a curve are summed by k_self64 with the full density,
+// the far field uses the density less its rigid part (see k_prep).  This is the
 // sum the reference's FMM approximates (stokesSolver.f:636-680; direct form
 // :1563-1584).  Sources are staged tile by tile in shared memory; a tile never
 // crosses a curve, so the mask test is one bit per tile and target.  blockIdx.y
@@ -165,12 +218,13 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
   const int N = G.N;
   const int split = blockIdx.y;
   const int i0 = blockIdx.x * (FAR_NT * FAR_TPT) + threadIdx.x;
-  int it[FAR_TPT];
+  int it[FAR_TPT], cv[FAR_TPT];
   double px[FAR_TPT], py[FAR_TPT], ax[FAR_TPT], ay[FAR_TPT];
 #pragma unroll
   for (int q = 0; q < FAR_TPT; ++q) {
     int i = i0 + q * FAR_NT;
     it[q] = i < N ? i : N - 1;
+    cv[q] = it[q] < G.nout ? 0 : 1 + (it[q] - G.nout) / G.n;
     double2 p = G.xy[it[q]];
     px[q] = p.x; py[q] = p.y; ax[q] = 0.0; ay[q] = 0.0;
   }
@@ -206,8 +260,8 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
     }
 #pragma unroll
     for (int q = 0; q < FAR_TPT; ++q) {
-      bool use = true;
-      if (MASK) use = !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
+      bool use = T.z != cv[q];
+      if (MASK) use = use && !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
       if (use) { ax[q] += tx[q]; ay[q] += ty[q]; }
     }
   }

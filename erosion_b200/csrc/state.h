@@ -146,7 +146,7 @@ struct State {
   int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32
 
   // work buffers
-  DBuf<double2> ws, partial, bd, pair_out;
+  DBuf<double2> ws, wrest, partial, bd, pair_out;
   DBuf<double> sigdotn;
   DBuf<double> d_xx, d_yy, d_den, d_rhs, d_r, d_w;
 

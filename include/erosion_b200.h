@@ -127,6 +127,10 @@ typedef struct {
   int64_t far32_launches;   /* FP32 far-field kernel launches                      */
   int64_t far32_pairs;      /* source-target pairs per FP32 far-field launch       */
   double true_residual_checks; /* FP64 true-residual evaluations (mixed mode)      */
+  double sweep_residual[8]; /* true residual after each refinement sweep          */
+  int64_t sweep_iterations[8]; /* GMRES iterations of each sweep                   */
+  int64_t floor_accepted;   /* 1: refinement stopped at the true-residual rounding
+                               floor (above tol) instead of below tol            */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
