@@ -394,32 +394,37 @@ __global__ void k_geom32(int ntile, const int4* __restrict__ tiles, const double
   }
 }
 
-// FP64 pairs within each curve (i != j): the self-interaction part of the
-// far-field sum for the mixed-precision operator.  CTA = (curve, <=256
-// targets); the curve streams through shared memory.
+// FP64 pairs within each curve (i != j), with the full density: the
+// self-interaction part of the far-field sum.  Task = (first target, count
+// <= 256, curve, source chunk); a curve longer than SELF_CHUNK is split into
+// chunks whose partial sums land in separate slots (out[slot*N + i]) and are
+// added in a fixed order by k_combine.
+constexpr int SELF_CHUNK = 512;
 __global__ void __launch_bounds__(256)
 k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tasks, double2* __restrict__ out) {
   __shared__ double4 sg[256];
   __shared__ double2 sw[256];
-  const int4 tk = tasks[blockIdx.x];   // target start, count, curve
-  const int c = tk.z;
+  const int4 tk = tasks[blockIdx.x];   // target start, count, curve, chunk
+  const int c = tk.z, chunk = tk.w;
   const int start = curve_start(G, c), len = curve_len(G, c);
+  const int kb = chunk * SELF_CHUNK, ke = min(len, kb + SELF_CHUNK);
   const int i = tk.x + threadIdx.x;
   const bool act = threadIdx.x < tk.y;
   const int ic = act ? i : tk.x;
   const double2 p = G.xy[ic];
   double ax = 0.0, ay = 0.0;
-  for (int k0 = 0; k0 < len; k0 += 256) {
+  for (int k0 = kb; k0 < ke; k0 += 256) {
     __syncthreads();
     const int kl = k0 + threadIdx.x;
-    if (kl < len) {
+    if (kl < ke) {
       int g = start + kl;
       double2 q = G.xy[g], nn = G.nrm[g];
       sg[threadIdx.x] = make_double4(q.x, q.y, nn.x, nn.y);
       sw[threadIdx.x] = ws[g];
     }
     __syncthreads();
-    const int kt = min(256, len - k0);
+    const int kt = min(256, ke - k0);
+#pragma unroll 4
     for (int j = 0; j < kt; ++j) {
       const double4 s = sg[j];
       const double2 a = sw[j];
@@ -433,7 +438,7 @@ k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ task
       ay = fma(cc, ry, ay);
     }
   }
-  if (act) out[i] = make_double2(ax, ay);
+  if (act) out[(size_t)chunk * G.N + i] = make_double2(ax, ay);
 }
 
 __global__ void k_ws32(int N, const double2* __restrict__ ws, float2* __restrict__ out) {
@@ -602,16 +607,25 @@ k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
 // 256-row chunk), warp per row.
 __global__ void __launch_bounds__(256)
 k_pc_apply_bodies(GeoDev G, const float* __restrict__ Binv, const double* __restrict__ v,
-                  const double2* __restrict__ tw, double* __restrict__ z) {
+                  const double2* __restrict__ tw, int ntw, double* __restrict__ z) {
   extern __shared__ float tv[];   // m entries of t_b
   const int b = blockIdx.x, n = G.n, m = 2 * n + 3;
   const long long sb = 2LL * G.nout + 2LL * n * b;      // sigma block of body b
   const long long cbk = 2LL * G.nout + 2LL * n * G.M + 3LL * b;
+  const size_t nb = (size_t)n * G.M;
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     double t;
-    if (r < n) t = v[sb + r] - tw[(size_t)b * n + r].x;
-    else if (r < 2 * n) t = v[sb + r] - tw[(size_t)b * n + (r - n)].y;
-    else t = v[cbk + (r - 2 * n)];
+    if (r < 2 * n) {
+      const int k = r < n ? r : r - n;
+      double cpl = 0.0;
+      for (int q = 0; q < ntw; ++q) {
+        const double2 v2 = tw[q * nb + (size_t)b * n + k];
+        cpl += r < n ? v2.x : v2.y;
+      }
+      t = v[sb + r] - cpl;
+    } else {
+      t = v[cbk + (r - 2 * n)];
+    }
     tv[r] = (float)t;
   }
   __syncthreads();
@@ -641,44 +655,65 @@ __global__ void k_pc_wall(GeoDev G, const double* __restrict__ v, double* __rest
 }
 
 // A_bw z_wall: the wall's trapezoid double layer at every body node, FP32
-// with the same tile-relative coordinates as k_far32.  One thread per body
-// node; the wall tiles stream through shared memory.
+// with the same tile-relative coordinates as k_far32.  Two body nodes per
+// thread; blockIdx.y selects a contiguous range of wall tiles and writes its
+// partial sums to out[y*nb + i] (added in order by k_pc_apply_bodies).
 __global__ void __launch_bounds__(256)
 k_pc_wall2body(int nout, int nb, const float4* __restrict__ src, const float2* __restrict__ tgt,
                const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
                const int4* __restrict__ tiles, int nwall_tiles, double2* __restrict__ out) {
   __shared__ float4 sg[WALL_TS];
   __shared__ float2 sw[WALL_TS];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = i < nb;
-  const int g = nout + (act ? i : nb - 1);
-  const float2 o = tgt[g];
-  const double2 a = anchor[g];
-  float hx = 0.f, lx = 0.f, hy = 0.f, ly = 0.f;
-  for (int ti = 0; ti < nwall_tiles; ++ti) {
+  const int tb = (int)((long long)blockIdx.y * nwall_tiles / gridDim.y);
+  const int te = (int)((long long)(blockIdx.y + 1) * nwall_tiles / gridDim.y);
+  float ox[2], oy[2], hx[2], lx[2], hy[2], ly[2];
+  double ax[2], ay[2];
+  int ii[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    int i = blockIdx.x * 512 + q * 256 + threadIdx.x;
+    ii[q] = i;
+    int g = nout + (i < nb ? i : nb - 1);
+    float2 o = tgt[g];
+    double2 a = anchor[g];
+    ox[q] = o.x; oy[q] = o.y; ax[q] = a.x; ay[q] = a.y;
+    hx[q] = lx[q] = hy[q] = ly[q] = 0.f;
+  }
+  for (int ti = tb; ti < te; ++ti) {
     const int4 T = tiles[ti];
     __syncthreads();
     if (threadIdx.x < T.y) { sg[threadIdx.x] = src[T.x + threadIdx.x]; sw[threadIdx.x] = ws32[T.x + threadIdx.x]; }
     __syncthreads();
     const double2 cs = tile_c[ti];
-    const float px = (float)(a.x - cs.x) + o.x, py = (float)(a.y - cs.y) + o.y;
-    float tx = 0.f, ty = 0.f;
+    float px[2], py[2], tx[2], ty[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      px[q] = (float)(ax[q] - cs.x) + ox[q];
+      py[q] = (float)(ay[q] - cs.y) + oy[q];
+      tx[q] = ty[q] = 0.f;
+    }
     for (int j = 0; j < T.y; ++j) {
       const float4 s = sg[j];
       const float2 w = sw[j];
-      float rx = px - s.x, ry = py - s.y;
-      float rho2 = fmaf(rx, rx, ry * ry);
-      float rdn = fmaf(rx, s.z, ry * s.w);
-      float rds = fmaf(rx, w.x, ry * w.y);
-      float inv = rcp_approx(rho2);
-      float c = (rdn * rds) * (inv * inv);
-      tx = fmaf(c, rx, tx);
-      ty = fmaf(c, ry, ty);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        float rx = px[q] - s.x, ry = py[q] - s.y;
+        float rho2 = fmaf(rx, rx, ry * ry);
+        float rdn = fmaf(rx, s.z, ry * s.w);
+        float rds = fmaf(rx, w.x, ry * w.y);
+        float inv = rcp_approx(rho2);
+        float c = (rdn * rds) * (inv * inv);
+        tx[q] = fmaf(c, rx, tx[q]);
+        ty[q] = fmaf(c, ry, ty[q]);
+      }
     }
-    two_sum_add(hx, lx, tx);
-    two_sum_add(hy, ly, ty);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) { two_sum_add(hx[q], lx[q], tx[q]); two_sum_add(hy[q], ly[q], ty[q]); }
   }
-  if (act) out[i] = make_double2((double)hx + (double)lx, (double)hy + (double)ly);
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    if (ii[q] < nb)
+      out[(size_t)blockIdx.y * nb + ii[q]] = make_double2((double)hx[q] + (double)lx[q], (double)hy[q] + (double)ly[q]);
 }
 
 // ---------------------------------------------------------------------------
@@ -952,7 +987,8 @@ constexpr int SR_CHUNK = 256;
 __global__ void __launch_bounds__(256)
 k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ partial, int nsplit,
           const int* __restrict__ tptr, const int* __restrict__ tpairs, const double2* __restrict__ pair_out,
-          const double* __restrict__ sigdotn, const double2* __restrict__ selfp, double* __restrict__ vel) {
+          const double* __restrict__ sigdotn, const double2* __restrict__ selfp, int nself,
+          double* __restrict__ vel) {
   __shared__ double4 sc[SR_CHUNK];   // cx, cy, stokeslet x, stokeslet y
   __shared__ double sr[SR_CHUNK];    // rotlet
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -965,8 +1001,11 @@ k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ 
     ux += v.x; uy += v.y;
   }
   if (selfp) {
-    double2 v = selfp[gc];
-    ux += v.x; uy += v.y;
+    const int ns = gc < G.nout ? nself : 1;   // only the wall is chunked
+    for (int q = 0; q < ns; ++q) {
+      double2 v = selfp[(size_t)q * G.N + gc];
+      ux += v.x; uy += v.y;
+    }
   }
   if (tptr) {
     for (int e = tptr[gc]; e < tptr[gc + 1]; ++e) {

@@ -195,11 +195,16 @@ static void build_tiles(State& s) {
   h2d(s.split_ptr.ensure(sp64.size()), sp64.data(), sp64.size(), s.st);
   h2d(s.split_ptr32.ensure(sp32.size()), sp32.data(), sp32.size(), s.st);
   s.partial.ensure((size_t)std::max(s.nsplit, s.nsplit32) * pr.N);
-  // self-curve tasks: (first target, count <= 256, curve)
+  // self-curve tasks: (first target, count <= 256, curve, source chunk)
   std::vector<int4> st;
+  s.n_self_slots = 1;
   for (int c = 0; c <= pr.M; ++c) {
     int start = c == 0 ? 0 : pr.nout + (c - 1) * pr.n, len = c == 0 ? pr.nout : pr.n;
-    for (int o = 0; o < len; o += 256) st.push_back(make_int4(start + o, std::min(256, len - o), c, 0));
+    int nch = (len + SELF_CHUNK - 1) / SELF_CHUNK;
+    if (c > 0) nch = 1;   // a body's self sum is short; only the wall is chunked
+    if (c == 0) s.n_self_slots = nch;
+    for (int ch = 0; ch < nch; ++ch)
+      for (int o = 0; o < len; o += 256) st.push_back(make_int4(start + o, std::min(256, len - o), c, ch));
   }
   s.n_self_tasks = (int)st.size();
   h2d(s.self_tasks.ensure(st.size()), st.data(), st.size(), s.st);
@@ -281,7 +286,7 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   s.ws32.ensure(N);
   s.tgt32.ensure(N);
   s.anchor.ensure(N);
-  s.selfsum.ensure(N);
+  s.selfsum.ensure((size_t)s.n_self_slots * N);
   s.tile_c.ensure(s.ntile);
   k_geom32<<<s.ntile, 256, 0, st>>>(s.ntile, s.tiles.p, s.xy.p, s.nrm.p, s.tile_c.p, s.src32.p, s.tgt32.p,
                                      s.anchor.p);
@@ -310,7 +315,11 @@ void setup_preconditioner(State& s) {
   EB_CK(cudaStreamSynchronize(s.st));
   s.pc_z.ensure(pr.ntot);
   s.pc_u.ensure(pr.ntot);
-  s.pc_tw.ensure((size_t)pr.M * n);
+  {
+    const int tblk = (int)nblk((long long)pr.M * n, 512);
+    s.pc_wsplit = std::max(1, std::min(s.nwall_tiles, (4 * g_num_sms + tblk - 1) / tblk));
+  }
+  s.pc_tw.ensure((size_t)s.pc_wsplit * pr.M * n);
   s.pc_ws32.ensure(pr.nout);
   s.pc_active = hbad == 0;   // a singular block leaves the solve unpreconditioned
 }
@@ -321,11 +330,12 @@ void apply_preconditioner(State& s, const double* v, double* z) {
   const int n = pr.n, m = 2 * n + 3, nb = n * pr.M;
   k_pc_wall<<<nblk(pr.nout, 256), 256, 0, s.st>>>(G, v, z, s.pc_ws32.p);
   EB_LAUNCH_CHECK();
-  k_pc_wall2body<<<nblk(nb, 256), 256, 0, s.st>>>(pr.nout, nb, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
-                                                  s.pc_ws32.p, s.tiles.p, s.nwall_tiles, s.pc_tw.p);
+  k_pc_wall2body<<<dim3(nblk(nb, 512), s.pc_wsplit), 256, 0, s.st>>>(pr.nout, nb, s.src32.p, s.tgt32.p, s.anchor.p,
+                                                                     s.tile_c.p, s.pc_ws32.p, s.tiles.p,
+                                                                     s.nwall_tiles, s.pc_tw.p);
   EB_LAUNCH_CHECK();
   dim3 g(pr.M, (unsigned)std::max(1, (m + 63) / 64));
-  k_pc_apply_bodies<<<g, 256, m * sizeof(float), s.st>>>(G, s.pcB.p, v, s.pc_tw.p, z);
+  k_pc_apply_bodies<<<g, 256, m * sizeof(float), s.st>>>(G, s.pcB.p, v, s.pc_tw.p, s.pc_wsplit, z);
   EB_LAUNCH_CHECK();
 }
 
@@ -389,7 +399,7 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
   }
   k_combine<<<nblk(pr.N, 256), 256, 0, st>>>(G, d_den, s.partial.p, nsplit, nr.npairs ? nr.tptr.p : nullptr,
                                              nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p,
-                                             s.selfsum.p, d_vel);
+                                             s.selfsum.p, s.n_self_slots, d_vel);
   EB_LAUNCH_CHECK();
   s.stats.matvecs++;
   s.stats.far32_pairs = s.far32_pairs;
