@@ -34,6 +34,7 @@ STATUS_NAMES = {
 
 PD = POINTER(c_double)
 PI64 = POINTER(c_int64)
+PF32 = POINTER(ctypes.c_float)
 
 
 class ErosionParams(ctypes.Structure):
@@ -52,7 +53,8 @@ class ErosionParams(ctypes.Structure):
         ("rhs_mode", c_int32),
         ("true_residual", c_int32),
         ("precond", c_int32),
-        ("reserved", c_int32 * 5),
+        ("learned_guess", c_int32),
+        ("reserved", c_int32 * 4),
         ("relax_tol", c_double),
     ]
 
@@ -78,12 +80,15 @@ class SolveStats(ctypes.Structure):
         ("sweep_residual", c_double * 8),
         ("sweep_iterations", c_int64 * 8),
         ("floor_accepted", c_int64),
+        ("guess_used", c_int64),
+        ("guess_residual", c_double * 3),
     ]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["sweep_residual"] = list(self.sweep_residual)[: max(self.sweeps, 0)]
         d["sweep_iterations"] = list(self.sweep_iterations)[: max(self.sweeps, 0)]
+        d["guess_residual"] = list(self.guess_residual)
         return d
 
 
@@ -100,12 +105,14 @@ class StepStats(ctypes.Structure):
 
     _fields_ = [("gmres_iterations", c_int64 * 2), ("bodies_deleted", c_int64),
                 ("ms_solve", c_double), ("ms_stress", c_double), ("ms_thetalen", c_double),
-                ("ms_total", c_double), ("max_residual", c_double), ("matau", c_double * 2)]
+                ("ms_total", c_double), ("max_residual", c_double), ("matau", c_double * 2),
+                ("guess_used", c_int64 * 2), ("guess_residual", c_double * 2)]
 
     def as_dict(self) -> dict:
         return {"gmres_iterations": list(self.gmres_iterations), "bodies_deleted": self.bodies_deleted,
                 "ms_solve": self.ms_solve, "ms_stress": self.ms_stress, "ms_thetalen": self.ms_thetalen,
-                "ms_total": self.ms_total, "max_residual": self.max_residual, "matau": list(self.matau)}
+                "ms_total": self.ms_total, "max_residual": self.max_residual, "matau": list(self.matau),
+                "guess_used": list(self.guess_used), "guess_residual": list(self.guess_residual)}
 
 
 # Every entry point declared in include/erosion_b200.h, with its signature.
@@ -138,6 +145,16 @@ SIGNATURES = {
                                         PD, PI64]),
     "erosion_getxy": (c_int, [c_int64, c_int64, PD, PD, PD, PD, PD, PD]),
     "erosion_stream": (ctypes.c_void_p, []),
+    "erosion_lw_features": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32]),
+    "erosion_lw_encode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PF32]),
+    "erosion_lw_decode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32, PD]),
+    "erosion_lw_init": (c_int, [ctypes.c_uint64]),
+    "erosion_lw_num_params": (c_int64, []),
+    "erosion_lw_get_params": (c_int, [PF32]),
+    "erosion_lw_set_params": (c_int, [PF32]),
+    "erosion_lw_loss_grad": (c_int, [PF32, PF32, c_int64, PD, PF32]),
+    "erosion_lw_train": (c_int, [PF32, PF32, c_int64, c_int64, c_int64, c_double, ctypes.c_uint64, PD]),
+    "erosion_lw_predict": (c_int, [PF32, c_int64, PF32]),
     "erosion_launch_count": (c_int64, []),
     "erosion_peak_tflops": (c_double, [c_int32]),
     "erosion_release": (None, []),

@@ -295,6 +295,57 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   s.geo_valid = true;
 }
 
+bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned) {
+  for (int q = 0; q < 3; ++q) s.stats.guess_residual[q] = -1.0;
+  s.stats.guess_residual[0] = 1.0;
+  const long long N = s.pr.ntot;
+  cudaStream_t st = s.st;
+  if (!learned) {
+    s.stats.guess_used = have_x ? 1 : 0;
+    return !have_x;
+  }
+  const double bnrm = device_norm(s, d_b, N);
+  if (!(bnrm > 0)) { s.stats.guess_used = have_x ? 1 : 0; return !have_x; }
+  double* r = s.d_r.ensure(N);
+  auto rel_res = [&](const double* x) {
+    apply_operator(s, x, r, 0);
+    k_bminus<<<nblk(N, 256), 256, 0, st>>>(d_b, r, N);
+    EB_LAUNCH_CHECK();
+    return device_norm(s, r, N) / bnrm;
+  };
+  double best = 1.0;
+  int used = 0;
+  if (have_x) {
+    const double rx = rel_res(d_x);
+    s.stats.guess_residual[1] = rx;
+    if (rx < best) { best = rx; used = 1; }
+  }
+  static DBuf<double> cand;
+  double* c = cand.ensure(N);
+  if (have_x) EB_CK(cudaMemcpyAsync(c, d_x, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  else EB_CK(cudaMemsetAsync(c, 0, N * sizeof(double), st));
+  if (lw_guess_current(s, c)) {
+    // the network predicts the bodies only: complete the wall density with
+    // Richardson sweeps on the wall rows (wall block ~ -1/2 I)
+    for (int it = 0; it < 3; ++it) {
+      rel_res(c);
+      k_wall_richardson<<<nblk(2LL * s.pr.nout, 256), 256, 0, st>>>(s.pr.nout, r, c);
+      EB_LAUNCH_CHECK();
+    }
+    const double rl = rel_res(c);
+    s.stats.guess_residual[2] = rl;
+    if (rl < best) {
+      best = rl;
+      used = 2;
+      EB_CK(cudaMemcpyAsync(d_x, c, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  if (used == 0) EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
+  EB_CK(cudaStreamSynchronize(st));
+  s.stats.guess_used = used;
+  return used == 0;
+}
+
 void setup_preconditioner(State& s) {
   const Problem& pr = s.pr;
   s.pc_active = false;
@@ -712,7 +763,13 @@ void setup_from_host(State& s, const Problem& pr, const double* xx, const double
 
 int solve_device_impl(State& s, double* d_den, bool x0_zero, int64_t* nits) {
   const Problem& pr = s.pr;
-  s.stats = erosion_solve_stats{};
+  {
+    const int64_t gu = s.stats.guess_used;
+    double gr[3] = {s.stats.guess_residual[0], s.stats.guess_residual[1], s.stats.guess_residual[2]};
+    s.stats = erosion_solve_stats{};
+    s.stats.guess_used = gu;
+    for (int q = 0; q < 3; ++q) s.stats.guess_residual[q] = gr[q];
+  }
   EB_CK(cudaEventRecord(s.e0, s.st));
   double* rhs = s.d_rhs.ensure(pr.ntot);
   build_rhs(s, rhs);
@@ -776,6 +833,12 @@ int erosion_solve(const erosion_params* p, int64_t npts, int64_t nbods, int64_t 
     for (long long i = 0; i < ntot && zero; ++i) zero = density[i] == 0.0;
     int rc = EROSION_OK;
     try {
+      s.stats = erosion_solve_stats{};
+      if (s.pr.P.learned_guess) {
+        double* rhs = s.d_rhs.ensure(ntot);
+        build_rhs(s, rhs);
+        zero = choose_initial_guess(s, rhs, dd, !zero, true);
+      }
       rc = solve_device_impl(s, dd, zero, nits);
     } catch (const Error& e) {
       if (e.code == EROSION_BAD_INPUT) {   // zero right-hand side: density zeroed

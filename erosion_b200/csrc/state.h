@@ -182,6 +182,13 @@ void build_rhs(State& s, double* d_rhs);
 // GMRES (SLATEC DGMRES semantics, CGS2 Arnoldi); returns EROSION_* status.
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
                 long long* iters, double* est);
+// Initial guess selection: candidates zero, the supplied d_x (have_x) and,
+// with learned, the network's guess; d_x receives the one with the smallest
+// FP64 residual.  Returns true when that is the zero vector.
+bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned);
+// Writes the learned density of every body into d_den (wall untouched);
+// false when no trained network exists.
+bool lw_guess_current(State& s, double* d_den);
 // Builds (or disables) the block preconditioner for the current geometry.
 void setup_preconditioner(State& s);
 // z = P^{-1} v (device vectors of length ntot).

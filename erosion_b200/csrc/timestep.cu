@@ -342,11 +342,13 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   setup_problem(s, pr, T.xx.p, T.yy.p);
   const long long ntot = s.pr.ntot;
   double* den = T.den[k].ensure(ntot);
-  bool zero = true;
-  if (sp.warm_start && T.den_ntot[k] == ntot) zero = false;
-  else EB_CK(cudaMemsetAsync(den, 0, ntot * sizeof(double), s.st));
+  const bool have_prev = sp.warm_start && T.den_ntot[k] == ntot;
+  if (!have_prev) EB_CK(cudaMemsetAsync(den, 0, ntot * sizeof(double), s.st));
   double* rhs = s.d_rhs.ensure(ntot);
   build_rhs(s, rhs);
+  const bool zero = choose_initial_guess(s, rhs, den, have_prev, sp.warm_start == 2);
+  T.stats.guess_used[k] = s.stats.guess_used;
+  T.stats.guess_residual[k] = s.stats.guess_used >= 0 ? s.stats.guess_residual[s.stats.guess_used] : -1;
   long long it = 0;
   double est = 0;
   int rc = gmres_solve(s, rhs, den, zero, s.pr.P.maxl, s.pr.P.tol, &it, &est);

@@ -101,7 +101,11 @@ typedef struct {
                            -2 I, wall-to-body coupling, exact inverse of every
                            body's (2 npts + 3) block in FP32.  The stopping test is
                            unchanged: ||b - A x||/||b|| <= tol                      */
-  int32_t reserved[5];
+  int32_t learned_guess; /* 1: also try the learned initial guess (the network of
+                           erosion_lw_train) and start GMRES from whichever of
+                           {learned, supplied density, zero} has the smallest FP64
+                           residual                                               */
+  int32_t reserved[4];
   double relax_tol;     /* mixed mode: GMRES switches to the FP32 far field once its
                            residual estimate is below relax_tol (relative);
                            0 selects the library default                           */
@@ -131,6 +135,8 @@ typedef struct {
   int64_t sweep_iterations[8]; /* GMRES iterations of each sweep                   */
   int64_t floor_accepted;   /* 1: refinement stopped at the true-residual rounding
                                floor (above tol) instead of below tol            */
+  int64_t guess_used;       /* initial guess: 0 zero, 1 supplied/previous, 2 learned */
+  double guess_residual[3]; /* ||b - A x0||/||b|| of each candidate (-1: not tried) */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
@@ -201,7 +207,9 @@ typedef struct {
                            that contain those slices)                            */
   int32_t warm_start;   /* 0: zero initial guess (the reference,
                            DensityStress.jl:45); 1: previous solve's density of
-                           the same stage when the body count is unchanged       */
+                           the same stage when the body count is unchanged;
+                           2: as 1 plus the learned guess, whichever of the
+                           candidates has the smallest residual                  */
   int32_t reserved[5];
 } erosion_step_params;
 
@@ -219,6 +227,9 @@ typedef struct {
   double ms_total;
   double max_residual;          /* largest GMRES estimate at exit             */
   double matau[2];              /* mean smoothed |tau| over bodies, per stage */
+  int64_t guess_used[2];        /* initial guess per stage: 0 zero, 1 previous,
+                                   2 learned                                  */
+  double guess_residual[2];     /* its relative residual ||b - A x0||/||b||   */
 } erosion_step_stats;
 
 /* One RK2 step of the theta-L state, host arrays, in place:
@@ -251,6 +262,36 @@ int64_t erosion_launch_count(void);
  * precision 0 = FP64, 1 = FP32, from a ~10 ms register-resident FMA loop
  * over every SM (the roofline denominator of the pair kernels). */
 double erosion_peak_tflops(int32_t precision);
+
+/* ------------------------------------------------------------------------
+ * Learned initial guess (no counterpart in the reference).  A network of
+ * 64 -> 256 -> 256 -> 256 -> 37 (GELU, BF16 weights, FP32 accumulation)
+ * maps per-body geometry features to the body's density (Fourier modes -8..8
+ * scaled by the body radius) and its stokeslet/rotlet strengths.
+ * ------------------------------------------------------------------------ */
+/* Per-body features of a geometry: feat[nbods*64]. */
+int erosion_lw_features(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                        const double* xx, const double* yy, float* feat);
+/* Per-body targets of a solved density: targ[nbods*37]. */
+int erosion_lw_encode(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                      const double* xx, const double* yy, const double* density, float* targ);
+/* Density (body entries, wall zero) of per-body targets. */
+int erosion_lw_decode(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                      const double* xx, const double* yy, const float* targ, double* density);
+/* Initialises the weights (He normal, seeded); erosion_lw_train does this too. */
+int erosion_lw_init(uint64_t seed);
+int64_t erosion_lw_num_params(void);
+int erosion_lw_get_params(float* out);
+int erosion_lw_set_params(const float* in);
+/* Mean squared error and its gradient with respect to every parameter for
+ * rows (x, y) used as given (no standardisation); for checking the backward
+ * kernels. */
+int erosion_lw_loss_grad(const float* x, const float* y, int64_t nsamples, double* loss, float* grads);
+/* Trains from scratch: standardisation from the data, then mini-batch Adam. */
+int erosion_lw_train(const float* feat, const float* targ, int64_t nsamples, int64_t epochs, int64_t batch,
+                     double lr, uint64_t seed, double* final_loss);
+/* Targets predicted by the trained network for raw features. */
+int erosion_lw_predict(const float* feat, int64_t nsamples, float* out);
 
 /* Releases every device buffer the library holds. */
 void erosion_release(void);
