@@ -19,6 +19,11 @@ def bf16(a: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def quantize(W: np.ndarray) -> np.ndarray:
+    """The weights as the products use them: FP32 master copy rounded to BF16."""
+    return bf16(W.astype(np.float32))
+
+
 def unpack(params: np.ndarray):
     out, o = [], 0
     for ni, no in LAYERS:
@@ -43,7 +48,7 @@ def gelu_grad(z):
 
 def loss_and_grad(params: np.ndarray, x: np.ndarray, y: np.ndarray):
     layers = unpack(params.astype(np.float64))
-    Wq = [bf16(W.astype(np.float32)) for W, _ in layers]
+    Wq = [quantize(W) for W, _ in layers]
     bs = [b.astype(np.float64) for _, b in layers]
     acts, pres = [x.astype(np.float64)], []
     h = acts[0]
