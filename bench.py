@@ -312,7 +312,9 @@ def main():
     far32_ms = s1["ms_far32"] - s0["ms_far32"]
     far32_n = s1["far32_launches"] - s0["far32_launches"]
     peak64 = L.erosion_peak_tflops(0)
-    peak32 = L.erosion_peak_tflops(1)
+    peak32_scalar = L.erosion_peak_tflops(1)
+    peak32_packed = L.erosion_peak_tflops(2)
+    peak32 = max(peak32_scalar, peak32_packed)   # the higher of scalar and two-lane FMA
     kernels = {}
     if far64_n:
         a = 20.0 * s1["far32_pairs"] / (far64_ms / far64_n * 1e-3) / 1e12
@@ -337,7 +339,10 @@ def main():
                 "frac": kernels[dom]["frac"] if dom else None, "traffic": traffic, "kernel": dom,
                 "algorithmic": "20 flops per source-target pair; pairs per launch = node pairs of distinct curves "
                                "less the barycentric near pairs (self-curve pairs run in k_self64)",
-                "peak_source": "measured FMA loop on this GPU (erosion_peak_tflops), vector pipe",
+                "peak_source": "measured FMA loop on this GPU (erosion_peak_tflops), vector pipe; FP32 = max of "
+                               "scalar and packed two-lane FMA",
+                "peaks_measured_tflops": {"fp64": peak64, "fp32_scalar": peak32_scalar, "fp32_packed": peak32_packed},
+                "launch_shapes": _lib.far_shapes(),
                 "kernels": kernels}
 
     # end to end through the host-array entry point (state in host memory)
@@ -378,6 +383,7 @@ def main():
     if args.compare_plain:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        sp0 = solve_stats()
         with torch.cuda.stream(stream):
             flush.zero_()
             e0.record(stream)
@@ -385,8 +391,11 @@ def main():
             e1.record(stream)
         torch.cuda.synchronize()
         pms = e0.elapsed_time(e1)
+        sp1 = solve_stats()
         plain = {"value": 1.0 / (pms * 1e-3) * world, "unit": "steps/s", "steps": 1,
                  "gmres_iterations_per_step": sum(stp["gmres_iterations"]),
+                 "step_breakdown_ms": {k: stp[k] for k in ("ms_solve", "ms_stress", "ms_thetalen", "ms_total")},
+                 "far64_ms": sp1["ms_far"] - sp0["ms_far"],
                  "form": "FP64 operator, no preconditioner, zero initial guess (the reference's algorithm)",
                  "speedup_of_value": value / (1.0 / (pms * 1e-3) * world)}
     if rank == 0:

@@ -157,6 +157,8 @@ SIGNATURES = {
     "erosion_lw_predict": (c_int, [PF32, c_int64, PF32]),
     "erosion_launch_count": (c_int64, []),
     "erosion_peak_tflops": (c_double, [c_int32]),
+    "erosion_set_far_shape": (c_int, [c_int32, c_int32]),
+    "erosion_get_far_shapes": (c_int, [POINTER(c_int32), POINTER(c_int32), PF32, POINTER(c_int32)]),
     "erosion_release": (None, []),
 }
 
@@ -227,3 +229,19 @@ def solve_stats() -> dict:
     s = SolveStats()
     load().erosion_get_solve_stats(ctypes.byref(s))
     return s.as_dict()
+
+
+def far_shapes() -> dict:
+    """The far-field launch shapes in use and the autotuner's timings."""
+    lib = load()
+    shape = (c_int32 * 2)()
+    nt = (c_int32 * 16)()
+    ms = (ctypes.c_float * 16)()
+    num = (c_int32 * 2)()
+    lib.erosion_get_far_shapes(shape, nt, ms, num)
+    out = {}
+    for kind, name in ((0, "fp64"), (1, "fp32")):
+        cands = [(nt[8 * kind + 2 * i], nt[8 * kind + 2 * i + 1]) for i in range(num[kind])]
+        out[name] = {"shape": cands[shape[kind]], "index": shape[kind],
+                     "tuned_ms": {f"{a}x{b}": round(ms[8 * kind + i], 4) for i, (a, b) in enumerate(cands)}}
+    return out

@@ -8,9 +8,9 @@
 namespace {
 
 // Problem-wide constants of the far-field kernels.
-constexpr int FAR_NT = 256;        // threads per CTA
-constexpr int FAR_TPT = 2;         // targets per thread (FP64)
-constexpr int FAR_TS = 256;        // sources per shared-memory tile (<= FAR_NT)
+constexpr int FAR_NT = 256;        // CTA shape (threads x targets per thread) that sets the tile
+constexpr int FAR_TPT = 2;         //   splits of the shear-stress and target sums
+constexpr int FAR_TS = 256;        // sources per shared-memory tile
 constexpr int WALL_TS = 32;        // wall nodes per tile (keeps FP32 offsets small)
 constexpr int NEAR_NT = 128;       // threads per CTA of the barycentric kernels
 constexpr int NEAR_TK = 128;       // source nodes per shared-memory tile
@@ -208,8 +208,8 @@ __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict
 // fixed order by k_combine.
 __device__ __forceinline__ double rcp_or_zero(double r2) { return r2 > 0.0 ? __drcp_rn(r2) : 0.0; }
 
-template <bool MASK>
-__global__ void __launch_bounds__(FAR_NT, 2)
+template <bool MASK, int NT, int TPT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
         const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
         double2* __restrict__ partial) {
@@ -217,12 +217,12 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
   __shared__ double2 sw[FAR_TS];
   const int N = G.N;
   const int split = blockIdx.y;
-  const int i0 = blockIdx.x * (FAR_NT * FAR_TPT) + threadIdx.x;
-  int it[FAR_TPT], cv[FAR_TPT];
-  double px[FAR_TPT], py[FAR_TPT], ax[FAR_TPT], ay[FAR_TPT];
+  const int i0 = blockIdx.x * (NT * TPT) + threadIdx.x;
+  int it[TPT], cv[TPT];
+  double px[TPT], py[TPT], ax[TPT], ay[TPT];
 #pragma unroll
-  for (int q = 0; q < FAR_TPT; ++q) {
-    int i = i0 + q * FAR_NT;
+  for (int q = 0; q < TPT; ++q) {
+    int i = i0 + q * NT;
     it[q] = i < N ? i : N - 1;
     cv[q] = it[q] < G.nout ? 0 : 1 + (it[q] - G.nout) / G.n;
     double2 p = G.xy[it[q]];
@@ -232,22 +232,22 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
   for (int ti = tb; ti < te; ++ti) {
     const int4 T = tiles[ti];
     __syncthreads();
-    if (threadIdx.x < T.y) {
-      int g = T.x + threadIdx.x;
+    for (int k = threadIdx.x; k < T.y; k += NT) {
+      int g = T.x + k;
       double2 q = G.xy[g], nn = G.nrm[g];
-      sg[threadIdx.x] = make_double4(q.x, q.y, nn.x, nn.y);
-      sw[threadIdx.x] = ws[g];
+      sg[k] = make_double4(q.x, q.y, nn.x, nn.y);
+      sw[k] = ws[g];
     }
     __syncthreads();
-    double tx[FAR_TPT], ty[FAR_TPT];
+    double tx[TPT], ty[TPT];
 #pragma unroll
-    for (int q = 0; q < FAR_TPT; ++q) { tx[q] = 0.0; ty[q] = 0.0; }
+    for (int q = 0; q < TPT; ++q) { tx[q] = 0.0; ty[q] = 0.0; }
 #pragma unroll 2
     for (int j = 0; j < T.y; ++j) {
       const double4 s = sg[j];
       const double2 a = sw[j];
 #pragma unroll
-      for (int q = 0; q < FAR_TPT; ++q) {
+      for (int q = 0; q < TPT; ++q) {
         double rx = px[q] - s.x, ry = py[q] - s.y;
         double rho2 = fma(rx, rx, ry * ry);
         double rdn = fma(rx, s.z, ry * s.w);
@@ -259,15 +259,15 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
       }
     }
 #pragma unroll
-    for (int q = 0; q < FAR_TPT; ++q) {
+    for (int q = 0; q < TPT; ++q) {
       bool use = T.z != cv[q];
       if (MASK) use = use && !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
       if (use) { ax[q] += tx[q]; ay[q] += ty[q]; }
     }
   }
 #pragma unroll
-  for (int q = 0; q < FAR_TPT; ++q) {
-    int i = i0 + q * FAR_NT;
+  for (int q = 0; q < TPT; ++q) {
+    int i = i0 + q * NT;
     if (i < N) partial[(size_t)split * N + i] = make_double2(ax[q], ay[q]);
   }
 }
@@ -276,12 +276,21 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
 // Far field, FP32 with compensated accumulation (the mixed-precision operator).
 // Same sum as k_far64 but over pairs of DIFFERENT curves only (a target's own
 // curve is evaluated in FP64 by k_self64) and without the near-masked pairs.
-// Each 256-source tile is summed in FP32 and folded into a two-sum (Knuth)
-// accumulator (hi, lo), so the rounding error grows with the tile length, not
-// with N.  Positions are absolute FP32 coordinates; the excluded pairs are
-// exactly the close ones where that would lose accuracy.
-constexpr int F32_NT = 256;
-constexpr int F32_TPT = 4;
+// Each tile is summed in FP32 and folded into a two-sum (Knuth) accumulator
+// (hi, lo), so the rounding error grows with the tile length, not with N.
+//
+// Coordinates: every node is stored as an FP32 offset from the FP64 centre of
+// its own tile (tiles never cross a curve and are at most one body or 32 wall
+// nodes long).  Per (target, source tile) the centre difference is formed in
+// FP64, so r = (c_t - c_s) + (o_t - o_s) is rounded relative to |r|, not to the
+// magnitude of the coordinates.
+//
+// Arithmetic: sm_100's packed FP32 instructions (two lanes per instruction,
+// each lane IEEE round-to-nearest exactly like the scalar instruction) process
+// two targets per instruction against one source, so every pair costs the same
+// rounded operations as the scalar form while the instruction count halves.
+// The source record is duplicated into both lanes when it is staged in shared
+// memory: (-x, -x, -y, -y), (nx, nx, ny, ny), (wx, wx, wy, wy).
 constexpr int F32_TS = 256;
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -298,81 +307,93 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t) {
   lo += e;
 }
 
-template <bool MASK>
-__global__ void __launch_bounds__(F32_NT, 2)
+template <bool MASK, int NT, int TPT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
         const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
         const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
         double2* __restrict__ partial) {
-  // Every node is stored as an FP32 offset from the FP64 centre of its own
-  // tile (tiles never cross a curve and are at most one body or 32 wall nodes
-  // long).  Per (target, source tile) the centre difference is formed in
-  // FP64, so r = (c_t - c_s) + (o_t - o_s) is rounded relative to |r|, not to
-  // the magnitude of the coordinates.
-  __shared__ float4 sg[F32_TS];
-  __shared__ float2 sw[F32_TS];
+  static_assert(TPT % 2 == 0, "targets are processed in lane pairs");
+  constexpr int TP = TPT / 2;
+  __shared__ float4 s_pos[F32_TS];
+  __shared__ float4 s_nrm[F32_TS];
+  __shared__ float4 s_den[F32_TS];
   const int split = blockIdx.y;
-  const int i0 = blockIdx.x * (F32_NT * F32_TPT) + threadIdx.x;
-  int it[F32_TPT], cv[F32_TPT];
-  double ax[F32_TPT], ay[F32_TPT];
-  float ox[F32_TPT], oy[F32_TPT], hx[F32_TPT], lx[F32_TPT], hy[F32_TPT], ly[F32_TPT];
+  const int i0 = blockIdx.x * (NT * TPT) + threadIdx.x;
+  int it[TPT], cv[TPT];
+  float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
 #pragma unroll
-  for (int q = 0; q < F32_TPT; ++q) {
-    int i = i0 + q * F32_NT;
+  for (int q = 0; q < TPT; ++q) {
+    int i = i0 + q * NT;
     it[q] = i < N ? i : N - 1;
     cv[q] = it[q] < nout ? 0 : 1 + (it[q] - nout) / n;
-    float2 p = tgt[it[q]];
-    double2 a = anchor[it[q]];
-    ox[q] = p.x; oy[q] = p.y; ax[q] = a.x; ay[q] = a.y;
     hx[q] = lx[q] = hy[q] = ly[q] = 0.f;
   }
   const int tb = split_ptr[split], te = split_ptr[split + 1];
   for (int ti = tb; ti < te; ++ti) {
     const int4 T = tiles[ti];
     __syncthreads();
-    if (threadIdx.x < T.y) {
-      sg[threadIdx.x] = src[T.x + threadIdx.x];
-      sw[threadIdx.x] = ws32[T.x + threadIdx.x];
+    for (int k = threadIdx.x; k < T.y; k += NT) {
+      const float4 a = src[T.x + k];
+      const float2 w = ws32[T.x + k];
+      s_pos[k] = make_float4(-a.x, -a.x, -a.y, -a.y);
+      s_nrm[k] = make_float4(a.z, a.z, a.w, a.w);
+      s_den[k] = make_float4(w.x, w.x, w.y, w.y);
     }
     __syncthreads();
     const double2 cs = tile_c[ti];
-    float px[F32_TPT], py[F32_TPT], tx[F32_TPT], ty[F32_TPT];
+    float2 PX[TP], PY[TP], TX[TP], TY[TP];
 #pragma unroll
-    for (int q = 0; q < F32_TPT; ++q) {
-      px[q] = (float)(ax[q] - cs.x) + ox[q];
-      py[q] = (float)(ay[q] - cs.y) + oy[q];
-      tx[q] = 0.f;
-      ty[q] = 0.f;
+    for (int p = 0; p < TP; ++p) {
+      const int q0 = it[2 * p], q1 = it[2 * p + 1];
+      const double2 a0 = anchor[q0], a1 = anchor[q1];
+      const float2 o0 = tgt[q0], o1 = tgt[q1];
+      PX[p] = make_float2((float)(a0.x - cs.x) + o0.x, (float)(a1.x - cs.x) + o1.x);
+      PY[p] = make_float2((float)(a0.y - cs.y) + o0.y, (float)(a1.y - cs.y) + o1.y);
+      TX[p] = make_float2(0.f, 0.f);
+      TY[p] = make_float2(0.f, 0.f);
     }
-#pragma unroll 4
+#pragma unroll 2
     for (int j = 0; j < T.y; ++j) {
-      const float4 s = sg[j];
-      const float2 a = sw[j];
+      const float4 A = s_pos[j], B = s_nrm[j], C = s_den[j];
+      const float2 msx = make_float2(A.x, A.y), msy = make_float2(A.z, A.w);
+      const float2 nx = make_float2(B.x, B.y), ny = make_float2(B.z, B.w);
+      const float2 wx = make_float2(C.x, C.y), wy = make_float2(C.z, C.w);
 #pragma unroll
-      for (int q = 0; q < F32_TPT; ++q) {
-        float rx = px[q] - s.x, ry = py[q] - s.y;
-        float rho2 = fmaf(rx, rx, ry * ry);
-        float rdn = fmaf(rx, s.z, ry * s.w);
-        float rds = fmaf(rx, a.x, ry * a.y);
-        float inv = rcp_approx(rho2);
-        float c = (rdn * rds) * (inv * inv);
-        tx[q] = fmaf(c, rx, tx[q]);
-        ty[q] = fmaf(c, ry, ty[q]);
+      for (int p = 0; p < TP; ++p) {
+        const float2 rx = __fadd2_rn(PX[p], msx);
+        const float2 ry = __fadd2_rn(PY[p], msy);
+        const float2 rho2 = __ffma2_rn(rx, rx, __fmul2_rn(ry, ry));
+        const float2 rdn = __ffma2_rn(rx, nx, __fmul2_rn(ry, ny));
+        const float2 rds = __ffma2_rn(rx, wx, __fmul2_rn(ry, wy));
+        const float2 inv = make_float2(rcp_approx(rho2.x), rcp_approx(rho2.y));
+        const float2 c = __fmul2_rn(__fmul2_rn(rdn, rds), __fmul2_rn(inv, inv));
+        TX[p] = __ffma2_rn(c, rx, TX[p]);
+        TY[p] = __ffma2_rn(c, ry, TY[p]);
       }
     }
 #pragma unroll
-    for (int q = 0; q < F32_TPT; ++q) {
+    for (int q = 0; q < TPT; ++q) {
       bool use = T.z != cv[q];
       if (MASK) use = use && !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
-      if (use) { two_sum_add(hx[q], lx[q], tx[q]); two_sum_add(hy[q], ly[q], ty[q]); }
+      const float tx = (q & 1) ? TX[q >> 1].y : TX[q >> 1].x;
+      const float ty = (q & 1) ? TY[q >> 1].y : TY[q >> 1].x;
+      if (use) { two_sum_add(hx[q], lx[q], tx); two_sum_add(hy[q], ly[q], ty); }
     }
   }
 #pragma unroll
-  for (int q = 0; q < F32_TPT; ++q) {
-    int i = i0 + q * F32_NT;
+  for (int q = 0; q < TPT; ++q) {
+    int i = i0 + q * NT;
     if (i < N) partial[(size_t)split * N + i] = make_double2((double)hx[q] + (double)lx[q], (double)hy[q] + (double)ly[q]);
   }
 }
+
+// Launch shapes the autotuner chooses from (threads per CTA, targets per
+// thread); solver.cu times each on the geometry at hand.
+struct FarShape { int nt, tpt; };
+constexpr FarShape kFar64Shapes[] = {{256, 2}, {128, 2}, {256, 1}, {128, 4}};
+constexpr FarShape kFar32Shapes[] = {{256, 4}, {256, 8}, {128, 8}, {128, 4}};
+constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4;
 
 // Tile centres (middle node) and, per node, the FP32 offset from its tile's
 // centre plus that centre (the target anchor of k_far32).  One CTA per tile.

@@ -31,6 +31,8 @@ void ensure_init(State& s) {
   EB_CK(cudaEventCreate(&s.e1));
   EB_CK(cudaEventCreate(&s.ef0));
   EB_CK(cudaEventCreate(&s.ef1));
+  EB_CK(cudaEventCreate(&s.et0));
+  EB_CK(cudaEventCreate(&s.et1));
   s.init = true;
 }
 
@@ -170,6 +172,21 @@ static void build_near(State& s, const std::vector<double2>& hxy, const std::vec
   EB_CK(cudaStreamSynchronize(st));   // host vectors go out of scope
 }
 
+// Split-K of the far-field sums: enough (target block, tile range) CTAs for
+// about 8 per SM; contiguous tile ranges of equal count.
+static int far_split_count(int N, int ntile, int targets_per_cta) {
+  int TB = (int)nblk(N, targets_per_cta);
+  int want = (int)std::ceil(8.0 * g_num_sms / TB);
+  return std::max(1, std::min(want, ntile));
+}
+
+static void upload_splits(State& s, DBuf<int>& buf, int ns) {
+  std::vector<int> sp(ns + 1);
+  for (int q = 0; q <= ns; ++q) sp[q] = (int)((long long)q * s.ntile / ns);
+  h2d(buf.ensure(sp.size()), sp.data(), sp.size(), s.st);
+  EB_CK(cudaStreamSynchronize(s.st));   // sp goes out of scope
+}
+
 static void build_tiles(State& s) {
   const Problem& pr = s.pr;
   std::vector<int4> tl;
@@ -180,21 +197,12 @@ static void build_tiles(State& s) {
   s.nwall_tiles = (int)tl.size();
   for (int b = 0; b < pr.M; ++b) add(pr.nout + b * pr.n, pr.n, 1 + b, FAR_TS);
   s.ntile = (int)tl.size();
-  auto splits = [&](int targets_per_cta, std::vector<int>& sp) {
-    int TB = (int)nblk(pr.N, targets_per_cta);
-    int want = (int)std::ceil(8.0 * g_num_sms / TB);
-    int ns = std::max(1, std::min(want, s.ntile));
-    sp.resize(ns + 1);
-    for (int q = 0; q <= ns; ++q) sp[q] = (int)((long long)q * s.ntile / ns);
-    return ns;
-  };
-  std::vector<int> sp64, sp32;
-  s.nsplit = splits(FAR_NT * FAR_TPT, sp64);
-  s.nsplit32 = splits(F32_NT * F32_TPT, sp32);
   h2d(s.tiles.ensure(tl.size()), tl.data(), tl.size(), s.st);
-  h2d(s.split_ptr.ensure(sp64.size()), sp64.data(), sp64.size(), s.st);
-  h2d(s.split_ptr32.ensure(sp32.size()), sp32.data(), sp32.size(), s.st);
-  s.partial.ensure((size_t)std::max(s.nsplit, s.nsplit32) * pr.N);
+  // tile splits of the shear-stress and target sums (the far-field kernels
+  // get theirs from plan_far, per launch shape)
+  s.nsplit = far_split_count(pr.N, s.ntile, FAR_NT * FAR_TPT);
+  upload_splits(s, s.split_ptr, s.nsplit);
+  s.partial.ensure((size_t)s.nsplit * pr.N);
   // self-curve tasks: (first target, count <= 256, curve, source chunk)
   std::vector<int4> st;
   s.n_self_slots = 1;
@@ -217,6 +225,131 @@ static void build_tiles(State& s) {
   }
   s.far32_pairs = (long long)pr.N * (pr.N - 1) - same - masked;
   EB_CK(cudaStreamSynchronize(s.st));
+}
+
+// ---------------------------------------------------------------------------
+// Far-field launch shapes and their autotuner.
+
+static int shape_targets(int kind, int shape) {
+  const FarShape sh = kind ? kFar32Shapes[shape] : kFar64Shapes[shape];
+  return sh.nt * sh.tpt;
+}
+
+static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Shapes[1].nt == 128 &&
+              kFar64Shapes[1].tpt == 2 && kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 1 &&
+              kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4, "launch_far's FP64 cases");
+static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].nt == 256 &&
+              kFar32Shapes[1].tpt == 8 && kFar32Shapes[2].nt == 128 && kFar32Shapes[2].tpt == 8 &&
+              kFar32Shapes[3].nt == 128 && kFar32Shapes[3].tpt == 4, "launch_far's FP32 cases");
+
+// One far-field launch of the given kind (0 FP64 on wrest, 1 FP32 on ws32)
+// and shape over the tile splits sp[0..nsplit].
+static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit) {
+  const Problem& pr = s.pr;
+  const Near& nr = s.near;
+  const GeoDev G = s.geo();
+  cudaStream_t st = s.st;
+  const bool mk = nr.npairs > 0;
+  const dim3 g((unsigned)nblk(pr.N, shape_targets(kind, shape)), (unsigned)nsplit);
+#define EB_FAR32(IDX, NT, TPT)                                                                                    \
+  case IDX:                                                                                                       \
+    if (mk)                                                                                                       \
+      k_far32<true, NT, TPT><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p, \
+                                               s.ws32.p, s.tiles.p, sp, nr.mask.p, nr.mw, s.partial.p);           \
+    else                                                                                                          \
+      k_far32<false, NT, TPT><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,           \
+                                                s.tile_c.p, s.ws32.p, s.tiles.p, sp, nullptr, 0, s.partial.p);    \
+    break;
+#define EB_FAR64(IDX, NT, TPT)                                                                                 \
+  case IDX:                                                                                                    \
+    if (mk)                                                                                                    \
+      k_far64<true, NT, TPT><<<g, NT, 0, st>>>(G, s.wrest.p, s.tiles.p, sp, nr.mask.p, nr.mw, s.partial.p);    \
+    else                                                                                                       \
+      k_far64<false, NT, TPT><<<g, NT, 0, st>>>(G, s.wrest.p, s.tiles.p, sp, nullptr, 0, s.partial.p);         \
+    break;
+  if (kind == 1) {
+    switch (shape) {
+      EB_FAR32(0, 256, 4)
+      EB_FAR32(1, 256, 8)
+      EB_FAR32(2, 128, 8)
+      EB_FAR32(3, 128, 4)
+      default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
+    }
+  } else {
+    switch (shape) {
+      EB_FAR64(0, 256, 2)
+      EB_FAR64(1, 128, 2)
+      EB_FAR64(2, 256, 1)
+      EB_FAR64(3, 128, 4)
+      default: throw Error(EROSION_BAD_INPUT, "unknown FP64 far-field shape");
+    }
+  }
+#undef EB_FAR32
+#undef EB_FAR64
+  EB_LAUNCH_CHECK();
+}
+
+// Problems below this many node pairs keep the first shape of each list (a
+// launch is a few microseconds; timing would cost more than it saves).
+constexpr double kTuneMinPairs = 2e8;
+
+// Chooses the launch shape of each far-field kernel for the current tiles.
+// A forced shape wins; otherwise, for large problems, every candidate is timed
+// (one warm-up and two timed launches on zeroed strengths, CUDA events on the
+// library stream) and the fastest kept.  The choice is cached per problem size
+// (N, tile count, masking), so an erosion run tunes once until a body is
+// deleted.
+static void plan_far(State& s) {
+  const Problem& pr = s.pr;
+  int maxsplit = s.nsplit;
+  for (int sh = 0; sh < kNumFar64Shapes; ++sh)
+    maxsplit = std::max(maxsplit, far_split_count(pr.N, s.ntile, shape_targets(0, sh)));
+  for (int sh = 0; sh < kNumFar32Shapes; ++sh)
+    maxsplit = std::max(maxsplit, far_split_count(pr.N, s.ntile, shape_targets(1, sh)));
+  s.partial.ensure((size_t)maxsplit * pr.N);
+  const int masked = s.near.npairs > 0;
+  const bool tune = (double)pr.N * (double)pr.N >= kTuneMinPairs;
+  const bool cached = s.tune_N == pr.N && s.tune_ntile == s.ntile && s.tune_masked == masked;
+  bool zeroed = false;
+  for (int kind = 0; kind < 2; ++kind) {
+    const int nsh = kind ? kNumFar32Shapes : kNumFar64Shapes;
+    int best = 0;
+    if (s.force_shape[kind] >= 0) {
+      best = s.force_shape[kind];
+    } else if (tune && cached && s.tuned_shape[kind] >= 0) {
+      best = s.tuned_shape[kind];
+    } else if (tune) {
+      if (!zeroed) {
+        EB_CK(cudaMemsetAsync(s.ws32.p, 0, sizeof(float2) * pr.N, s.st));
+        EB_CK(cudaMemsetAsync(s.wrest.p, 0, sizeof(double2) * pr.N, s.st));
+        zeroed = true;
+      }
+      float bestms = 1e30f;
+      for (int sh = 0; sh < nsh; ++sh) {
+        const int ns = far_split_count(pr.N, s.ntile, shape_targets(kind, sh));
+        upload_splits(s, s.split_tune, ns);
+        launch_far(s, kind, sh, s.split_tune.p, ns);
+        float ms = 1e30f;
+        for (int r = 0; r < 2; ++r) {
+          EB_CK(cudaEventRecord(s.et0, s.st));
+          launch_far(s, kind, sh, s.split_tune.p, ns);
+          EB_CK(cudaEventRecord(s.et1, s.st));
+          EB_CK(cudaEventSynchronize(s.et1));
+          float t = 0;
+          EB_CK(cudaEventElapsedTime(&t, s.et0, s.et1));
+          ms = std::min(ms, t);
+        }
+        s.tune_ms[kind][sh] = ms;
+        if (ms < bestms) { bestms = ms; best = sh; }
+      }
+      s.tuned_shape[kind] = best;
+    }
+    s.far_shape[kind] = best;
+    const int ns = far_split_count(pr.N, s.ntile, shape_targets(kind, best));
+    if (kind == 1) { s.nsplit32 = ns; upload_splits(s, s.split_ptr32, ns); }
+    else { s.nsplit64t = ns; upload_splits(s, s.split_ptr64t, ns); }
+  }
+  if (tune) { s.tune_N = pr.N; s.tune_ntile = s.ntile; s.tune_masked = masked; }
 }
 
 void setup_problem(State& s, const Problem& in, const double* d_xx, const double* d_yy) {
@@ -291,6 +424,8 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   k_geom32<<<s.ntile, 256, 0, st>>>(s.ntile, s.tiles.p, s.xy.p, s.nrm.p, s.tile_c.p, s.src32.p, s.tgt32.p,
                                      s.anchor.p);
   EB_LAUNCH_CHECK();
+  harvest_far_timing(s);
+  plan_far(s);
   setup_preconditioner(s);
   s.geo_valid = true;
 }
@@ -408,33 +543,16 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
   cudaStream_t st = s.st;
   k_prep<<<pr.M + 1, 256, 0, st>>>(G, d_den, s.ws.p, s.wrest.p, s.ws32.p, d_vel, s.sigdotn.p, pr.P.ibary == 1);
   EB_LAUNCH_CHECK();
-  int nsplit;
-  if (prec == 1) {
-    dim3 fg(nblk(pr.N, F32_NT * F32_TPT), s.nsplit32);
-    EB_CK(cudaEventRecord(s.ef0, st));
-    if (nr.npairs > 0)
-      k_far32<true><<<fg, F32_NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
-                                           s.ws32.p, s.tiles.p, s.split_ptr32.p, nr.mask.p, nr.mw, s.partial.p);
-    else
-      k_far32<false><<<fg, F32_NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p,
-                                            s.ws32.p, s.tiles.p, s.split_ptr32.p, nullptr, 0, s.partial.p);
-    EB_LAUNCH_CHECK();
-    EB_CK(cudaEventRecord(s.ef1, st));
-    s.far_kind = 1;
-    nsplit = s.nsplit32;
+  const int kind = prec == 1 ? 1 : 0;
+  const int nsplit = kind ? s.nsplit32 : s.nsplit64t;
+  EB_CK(cudaEventRecord(s.ef0, st));
+  launch_far(s, kind, s.far_shape[kind], kind ? s.split_ptr32.p : s.split_ptr64t.p, nsplit);
+  EB_CK(cudaEventRecord(s.ef1, st));
+  s.far_kind = kind;
+  if (kind == 1) {
     s.stats.matvecs_fp32++;
     s.stats.far32_launches++;
   } else {
-    dim3 fg(nblk(pr.N, FAR_NT * FAR_TPT), s.nsplit);
-    EB_CK(cudaEventRecord(s.ef0, st));
-    if (nr.npairs > 0)
-      k_far64<true><<<fg, FAR_NT, 0, st>>>(G, s.wrest.p, s.tiles.p, s.split_ptr.p, nr.mask.p, nr.mw, s.partial.p);
-    else
-      k_far64<false><<<fg, FAR_NT, 0, st>>>(G, s.wrest.p, s.tiles.p, s.split_ptr.p, nullptr, 0, s.partial.p);
-    EB_LAUNCH_CHECK();
-    EB_CK(cudaEventRecord(s.ef1, st));
-    s.far_kind = 0;
-    nsplit = s.nsplit;
     s.stats.far_launches++;
   }
   k_self64<<<s.n_self_tasks, 256, 0, st>>>(G, s.ws.p, s.self_tasks.p, s.selfsum.p);
@@ -958,6 +1076,35 @@ void* erosion_stream(void) {
 
 int64_t erosion_launch_count(void) { return (int64_t)g_launches; }
 
+int erosion_set_far_shape(int32_t kind, int32_t shape) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  const int nsh = kind == 0 ? kNumFar64Shapes : kNumFar32Shapes;
+  if ((kind != 0 && kind != 1) || shape < -1 || shape >= nsh) {
+    s.status = EROSION_BAD_INPUT;
+    s.err = "unknown far-field kernel kind or shape";
+    return EROSION_BAD_INPUT;
+  }
+  s.force_shape[kind] = shape;
+  return EROSION_OK;
+}
+
+int erosion_get_far_shapes(int32_t* shape, int32_t* nt_tpt, float* ms, int32_t* num_shapes) {
+  State& s = state();
+  std::lock_guard<std::mutex> lk(s.mu);
+  for (int kind = 0; kind < 2; ++kind) {
+    const int nsh = kind ? kNumFar32Shapes : kNumFar64Shapes;
+    if (shape) shape[kind] = s.far_shape[kind];
+    if (num_shapes) num_shapes[kind] = nsh;
+    for (int i = 0; i < nsh; ++i) {
+      const FarShape sh = kind ? kFar32Shapes[i] : kFar64Shapes[i];
+      if (nt_tpt) { nt_tpt[8 * kind + 2 * i] = sh.nt; nt_tpt[8 * kind + 2 * i + 1] = sh.tpt; }
+      if (ms) ms[8 * kind + i] = s.tune_ms[kind][i] < 1e29f ? s.tune_ms[kind][i] : 0.f;
+    }
+  }
+  return EROSION_OK;
+}
+
 int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs) {
   State& s = state();
   std::lock_guard<std::mutex> lk(s.mu);
@@ -984,7 +1131,8 @@ void erosion_release(void) {
   s.zcap = 0;
   s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
   s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
-  s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release();
+  s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release();
+  s.split_tune.release(); s.tune_N = -1; s.tuned_shape[0] = s.tuned_shape[1] = -1;
   s.dker_body_n = s.dker_wall_n = -1;
   s.geo_valid = false;
 }

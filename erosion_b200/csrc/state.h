@@ -125,8 +125,16 @@ struct State {
 
   // far field
   DBuf<int4> tiles;
-  DBuf<int> split_ptr, split_ptr32;
-  int nsplit = 0, nsplit32 = 0, ntile = 0;
+  DBuf<int> split_ptr, split_ptr32, split_ptr64t, split_tune;
+  int nsplit = 0, nsplit32 = 0, nsplit64t = 0, ntile = 0;
+  // far-field launch shapes: index into the candidate lists of kernels.cuh
+  // (kind 0 FP64, 1 FP32), chosen by the autotuner or forced by the caller
+  int far_shape[2] = {0, 0};
+  int force_shape[2] = {-1, -1};
+  int tuned_shape[2] = {-1, -1};
+  int tune_N = -1, tune_ntile = -1, tune_masked = -1;
+  float tune_ms[2][8] = {};
+  cudaEvent_t et0 = nullptr, et1 = nullptr;
   // mixed precision: FP32 geometry, strengths, self-curve tasks and sums
   DBuf<float4> src32;
   DBuf<float2> ws32, tgt32;

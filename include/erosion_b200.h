@@ -259,9 +259,27 @@ void* erosion_stream(void);
 int64_t erosion_launch_count(void);
 
 /* Measured vector FMA throughput of this GPU in TFLOP/s (2 flops per FMA):
- * precision 0 = FP64, 1 = FP32, from a ~10 ms register-resident FMA loop
+ * precision 0 = FP64, 1 = FP32 scalar FMA, 2 = FP32 packed two-lane FMA
+ * (sm_100's f32x2 instructions), from a ~10 ms register-resident FMA loop
  * over every SM (the roofline denominator of the pair kernels). */
 double erosion_peak_tflops(int32_t precision);
+
+/* Far-field launch shapes (extended API; the reference's FMM has no
+ * counterpart).  Each far-field kernel has a list of candidate CTA shapes
+ * (threads per CTA x targets per thread); by default an autotuner times
+ * every candidate on the geometry at hand the first time a problem of that
+ * size is set up (problems above 2e8 node pairs) and keeps the fastest.
+ * erosion_set_far_shape(kind, shape) forces candidate 'shape' (kind 0 = the
+ * FP64 kernel, 1 = the FP32 kernel) from the next set-up on; shape = -1
+ * returns to the autotuner.  Returns EROSION_BAD_INPUT for an unknown kind
+ * or shape. */
+int erosion_set_far_shape(int32_t kind, int32_t shape);
+
+/* The shapes in use: shape[kind] = candidate index; nt_tpt[8*kind + 2*i ..]
+ * = (threads, targets per thread) of candidate i (num_shapes[kind] of them,
+ * at most 4, capacity 16 entries); ms[8*kind + i] = the autotuner's time of
+ * candidate i in milliseconds (0 when not timed).  Any pointer may be NULL. */
+int erosion_get_far_shapes(int32_t* shape, int32_t* nt_tpt, float* ms, int32_t* num_shapes);
 
 /* ------------------------------------------------------------------------
  * Learned initial guess (no counterpart in the reference).  A network of
