@@ -128,6 +128,8 @@ SIGNATURES = {
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, PI64]),
     "erosion_get_solve_stats": (None, [POINTER(SolveStats)]),
     "erosion_matvec": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD]),
+    "erosion_matvec_noalloc": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "erosion_rhs": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD]),
     "erosion_geometry": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD] + [PD] * 12),
     "erosion_shear_stress": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD, PD]),

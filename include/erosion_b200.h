@@ -156,6 +156,27 @@ void erosion_get_solve_stats(erosion_solve_stats* s);
 int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                    const double* xx, const double* yy, const double* density, double* vel);
 
+/* The trapezoid-rule boundary operator (erosion_matvec with ibary = 0 and
+ * precision = 0) for callers that cannot allocate GPU memory — a caller whose
+ * runtime owns all device memory or whose device memory is reserved up front,
+ * running its own iterative solver around this operator.  No counterpart in
+ * the reference (an addition of this library).  Inputs and output are DEVICE
+ * pointers (d_xx, d_yy: [npts*nbods] body nodes; d_den, d_vel: [2*npts*nbods
+ * + 3*nbods + 2*nouter]); the kernels run on 'stream' (a cudaStream_t, NULL
+ * = the legacy default stream) and the call returns without waiting for them.
+ * It allocates no device memory: every intermediate lives in one fixed 24 MiB
+ * array that is part of the library on every GPU that loads it, which limits
+ * the size to nouter <= 4096, npts <= 512, nbods <= 128 and nouter +
+ * npts*nbods <= 32768 (larger sizes, ibary != 0 or precision != 0 return
+ * EROSION_BAD_INPUT).  The first call on a device looks up that array's
+ * device address; make it before capturing any stream.  Calls share the
+ * array: calls whose kernels overlap on the GPU race and must be ordered by
+ * the caller.  Inputs are not checked for finiteness or for bodies inside the
+ * wall. */
+int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
+                           const double* d_xx, const double* d_yy, const double* d_den, double* d_vel,
+                           void* stream);
+
 /* The right-hand side of bd_condition (stokesSolver.f:208-314). */
 int erosion_rhs(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                 const double* xx, const double* yy, double* rhs);
