@@ -317,10 +317,17 @@ def main():
     peak32 = max(peak32_scalar, peak32_packed)   # the higher of scalar and two-lane FMA
     kernels = {}
     if far64_n:
-        a = 20.0 * s1["far32_pairs"] / (far64_ms / far64_n * 1e-3) / 1e12
+        a = 20.0 * s1["far64_pairs"] / (far64_ms / far64_n * 1e-3) / 1e12
         kernels["k_far64"] = {"launches": far64_n, "ms_total": far64_ms, "ms_avg": far64_ms / far64_n,
-                              "pairs_per_launch": s1["far32_pairs"], "achieved_tflops": a, "peak_tflops": peak64,
+                              "pairs_per_launch": s1["far64_pairs"], "achieved_tflops": a, "peak_tflops": peak64,
                               "frac": a / peak64, "share_of_timed": far64_ms / ms}
+    farw_ms = s1["ms_farw"] - s0["ms_farw"]
+    farw_n = s1["farw_launches"] - s0["farw_launches"]
+    if farw_n:
+        a = 20.0 * s1["farw_pairs"] / (farw_ms / farw_n * 1e-3) / 1e12
+        kernels["k_far64_wall_sources"] = {"launches": farw_n, "ms_total": farw_ms, "ms_avg": farw_ms / farw_n,
+                                           "pairs_per_launch": s1["farw_pairs"], "achieved_tflops": a,
+                                           "peak_tflops": peak64, "frac": a / peak64, "share_of_timed": farw_ms / ms}
     if far32_n:
         pairs32 = s1["far32_pairs"]
         a = 20.0 * pairs32 / (far32_ms / far32_n * 1e-3) / 1e12
@@ -334,11 +341,13 @@ def main():
             traffic = json.load(f).get(f"{args.workload}:{dom}") or json.load(open(TRAFFIC_FILE)).get(args.workload)
     except Exception:
         pass
-    roofline = {"bound": "fp64" if dom == "k_far64" else "fp32", "achieved": kernels[dom]["achieved_tflops"] if dom else None,
+    roofline = {"bound": "fp32" if dom == "k_far32" else "fp64", "achieved": kernels[dom]["achieved_tflops"] if dom else None,
                 "peak": kernels[dom]["peak_tflops"] if dom else None, "unit": "TFLOP/s",
                 "frac": kernels[dom]["frac"] if dom else None, "traffic": traffic, "kernel": dom,
-                "algorithmic": "20 flops per source-target pair; pairs per launch = node pairs of distinct curves "
-                               "less the barycentric near pairs (self-curve pairs run in k_self64)",
+                "algorithmic": "20 flops per source-target pair; pairs per launch: k_far64 = node pairs of distinct "
+                               "curves less the barycentric near pairs (self-curve pairs run in k_self64); in the "
+                               "mixed operator k_far32 takes the body-source pairs and k_far64_wall_sources the "
+                               "wall-source pairs",
                 "peak_source": "measured FMA loop on this GPU (erosion_peak_tflops), vector pipe; FP32 = max of "
                                "scalar and packed two-lane FMA",
                 "peaks_measured_tflops": {"fp64": peak64, "fp32_scalar": peak32_scalar, "fp32_packed": peak32_packed},

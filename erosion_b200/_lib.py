@@ -82,6 +82,10 @@ class SolveStats(ctypes.Structure):
         ("floor_accepted", c_int64),
         ("guess_used", c_int64),
         ("guess_residual", c_double * 3),
+        ("far64_pairs", c_int64),
+        ("ms_farw", c_double),
+        ("farw_launches", c_int64),
+        ("farw_pairs", c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -237,13 +241,14 @@ def far_shapes() -> dict:
     """The far-field launch shapes in use and the autotuner's timings."""
     lib = load()
     shape = (c_int32 * 2)()
-    nt = (c_int32 * 16)()
+    desc = (c_int32 * 24)()
     ms = (ctypes.c_float * 16)()
     num = (c_int32 * 2)()
-    lib.erosion_get_far_shapes(shape, nt, ms, num)
+    lib.erosion_get_far_shapes(shape, desc, ms, num)
     out = {}
     for kind, name in ((0, "fp64"), (1, "fp32")):
-        cands = [(nt[8 * kind + 2 * i], nt[8 * kind + 2 * i + 1]) for i in range(num[kind])]
-        out[name] = {"shape": cands[shape[kind]], "index": shape[kind],
-                     "tuned_ms": {f"{a}x{b}": round(ms[8 * kind + i], 4) for i, (a, b) in enumerate(cands)}}
+        cands = [tuple(desc[12 * kind + 3 * i: 12 * kind + 3 * i + 3]) for i in range(num[kind])]
+        label = lambda c: f"{c[0]}x{c[1]}" + ("-newton" if c[2] else "")
+        out[name] = {"shape": label(cands[shape[kind]]), "index": shape[kind],
+                     "tuned_ms": {label(c): round(ms[8 * kind + i], 4) for i, c in enumerate(cands)}}
     return out

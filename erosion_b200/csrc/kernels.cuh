@@ -208,7 +208,24 @@ __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict
 // fixed order by k_combine.
 __device__ __forceinline__ double rcp_or_zero(double r2) { return r2 > 0.0 ? __drcp_rn(r2) : 0.0; }
 
-template <bool MASK, int NT, int TPT>
+// 1/r2 for r2 > 0 by Newton-Raphson: the FP32 hardware reciprocal estimate
+// (relative error ~2^-23), refined twice by y <- y + y (1 - r2 y) in FP64
+// (quadratic convergence: ~2^-46, then below FP64 rounding).  r2 spans
+// ~1e-10..1e2 here, well inside FP32's normal range.  Not correctly rounded
+// (a last-bit difference from the division), which the operator's 1e-11
+// parity bound absorbs.
+__device__ __forceinline__ double rcp_newton(double r2) {
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(r2)));
+  double y = (double)yf;
+  double e = fma(-r2, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-r2, y, 1.0);
+  y = fma(y, e, y);
+  return r2 > 0.0 ? y : 0.0;
+}
+
+template <bool MASK, int NT, int TPT, int RCP>
 __global__ void __launch_bounds__(NT, 512 / NT)
 k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
         const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
@@ -252,7 +269,7 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
         double rho2 = fma(rx, rx, ry * ry);
         double rdn = fma(rx, s.z, ry * s.w);
         double rds = fma(rx, a.x, ry * a.y);
-        double inv = rcp_or_zero(rho2);
+        double inv = RCP ? rcp_newton(rho2) : rcp_or_zero(rho2);
         double c = rdn * rds * inv * inv;
         tx[q] = fma(c, rx, tx[q]);
         ty[q] = fma(c, ry, ty[q]);
@@ -390,9 +407,11 @@ k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __
 
 // Launch shapes the autotuner chooses from (threads per CTA, targets per
 // thread); solver.cu times each on the geometry at hand.
-struct FarShape { int nt, tpt; };
-constexpr FarShape kFar64Shapes[] = {{256, 2}, {128, 2}, {256, 1}, {128, 4}};
-constexpr FarShape kFar32Shapes[] = {{256, 4}, {256, 8}, {128, 8}, {128, 4}};
+// For the FP64 kernel, rcp selects the reciprocal: 0 the division
+// (__drcp_rn), 1 rcp_newton.
+struct FarShape { int nt, tpt, rcp; };
+constexpr FarShape kFar64Shapes[] = {{256, 2, 0}, {256, 2, 1}, {256, 1, 1}, {128, 4, 1}};
+constexpr FarShape kFar32Shapes[] = {{256, 4, 0}, {256, 8, 0}, {128, 8, 0}, {128, 4, 0}};
 constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4;
 
 // Tile centres (middle node) and, per node, the FP32 offset from its tile's

@@ -225,7 +225,7 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
     }
     k_prep<<<M + 1, 256, 0, st>>>(G, d_den, ws, wrest, ws32, d_vel, sigdotn, 0);
     EB_LAUNCH_CHECK();
-    k_far64<false, FAR_NT, FAR_TPT><<<dim3((unsigned)TB, (unsigned)nsplit), FAR_NT, 0, st>>>(
+    k_far64<false, FAR_NT, FAR_TPT, 0><<<dim3((unsigned)TB, (unsigned)nsplit), FAR_NT, 0, st>>>(
         G, wrest, tiles, split_ptr, nullptr, 0, partial);
     EB_LAUNCH_CHECK();
     k_self64<<<ntask, 256, 0, st>>>(G, ws, tasks, selfsum);

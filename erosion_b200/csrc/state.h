@@ -108,7 +108,7 @@ struct State {
   bool init = false;
   int device = -1;
   cudaStream_t st = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr, ef0 = nullptr, ef1 = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, ef0 = nullptr, ef1 = nullptr, ew0 = nullptr, ew1 = nullptr;
 
   Problem pr;
   bool geo_valid = false;
@@ -125,8 +125,9 @@ struct State {
 
   // far field
   DBuf<int4> tiles;
-  DBuf<int> split_ptr, split_ptr32, split_ptr64t, split_tune;
-  int nsplit = 0, nsplit32 = 0, nsplit64t = 0, ntile = 0;
+  DBuf<int> split_ptr, split_ptr32, split_ptr64t, split_ptrw, split_tune;
+  int nsplit = 0, nsplit32 = 0, nsplit64t = 0, nsplitw = 0, ntile = 0;
+  long long far64_pairs = 0, farw_pairs = 0;   // pairs per full FP64 / wall-source launch
   // far-field launch shapes: index into the candidate lists of kernels.cuh
   // (kind 0 FP64, 1 FP32), chosen by the autotuner or forced by the caller
   int far_shape[2] = {0, 0};
@@ -167,6 +168,7 @@ struct State {
   size_t h_pinned_cap = 0;
 
   erosion_solve_stats stats{};
+  bool farw_pending = false;  // ew0/ew1 bracket a wall-source FP64 launch not yet harvested
   bool far_pending = false;   // ef0/ef1 bracket a far-field launch not yet harvested
 
   GeoDev geo() const {

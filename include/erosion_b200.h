@@ -137,6 +137,11 @@ typedef struct {
                                floor (above tol) instead of below tol            */
   int64_t guess_used;       /* initial guess: 0 zero, 1 supplied/previous, 2 learned */
   double guess_residual[3]; /* ||b - A x0||/||b|| of each candidate (-1: not tried) */
+  int64_t far64_pairs;      /* source-target pairs per full FP64 far-field launch   */
+  double ms_farw;           /* mixed operator: device time of the FP64 wall-source
+                               far-field launches                                  */
+  int64_t farw_launches;    /* their count                                         */
+  int64_t farw_pairs;       /* wall-source pairs per such launch                   */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
@@ -151,8 +156,9 @@ void erosion_get_solve_stats(erosion_solve_stats* s);
 
 /* One application of the boundary operator (host arrays) — the reference's
  * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm;
- * precision = 1 applies the mixed-precision operator (FP32 far field between
- * distinct curves, FP64 elsewhere). */
+ * precision = 1 applies the mixed-precision operator (FP32 far field from body
+ * sources to the nodes of other curves, FP64 elsewhere, the wall's sources
+ * included). */
 int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                    const double* xx, const double* yy, const double* density, double* vel);
 
@@ -296,11 +302,12 @@ double erosion_peak_tflops(int32_t precision);
  * or shape. */
 int erosion_set_far_shape(int32_t kind, int32_t shape);
 
-/* The shapes in use: shape[kind] = candidate index; nt_tpt[8*kind + 2*i ..]
- * = (threads, targets per thread) of candidate i (num_shapes[kind] of them,
- * at most 4, capacity 16 entries); ms[8*kind + i] = the autotuner's time of
- * candidate i in milliseconds (0 when not timed).  Any pointer may be NULL. */
-int erosion_get_far_shapes(int32_t* shape, int32_t* nt_tpt, float* ms, int32_t* num_shapes);
+/* The shapes in use: shape[kind] = candidate index; desc[12*kind + 3*i ..] =
+ * (threads, targets per thread, reciprocal: 0 division, 1 Newton-Raphson from
+ * the FP32 estimate) of candidate i (num_shapes[kind] of them, at most 4,
+ * capacity 24 entries); ms[8*kind + i] = the autotuner's time of candidate i
+ * in milliseconds (0 when not timed).  Any pointer may be NULL. */
+int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* num_shapes);
 
 /* ------------------------------------------------------------------------
  * Learned initial guess (no counterpart in the reference).  A network of
