@@ -96,6 +96,20 @@ class SolveStats(ctypes.Structure):
         return d
 
 
+class BatchStats(ctypes.Structure):
+    """Mirror of ``erosion_batch_stats``."""
+
+    _fields_ = [("geometries", c_int64), ("rounds", c_int64), ("iterations", c_int64), ("graph_captures", c_int64),
+                ("ms_total", c_double), ("pairs64_per_round", c_double), ("pairs32_per_round", c_double),
+                ("pairs64_total", c_double), ("pairs32_total", c_double), ("max_true_residual", c_double),
+                ("shape64", c_int64), ("shape32", c_int64), ("tune_ms", ctypes.c_float * 8)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["tune_ms"] = list(self.tune_ms)
+        return d
+
+
 class StepParams(ctypes.Structure):
     """Mirror of ``erosion_step_params``."""
 
@@ -131,6 +145,8 @@ SIGNATURES = {
     "erosion_solve_device": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, PI64]),
     "erosion_get_solve_stats": (None, [POINTER(SolveStats)]),
+    "erosion_solve_batch": (c_int, [POINTER(ErosionParams), c_int32, PI64, PI64, PI64, PD, PD, PD, PI64]),
+    "erosion_get_batch_stats": (None, [POINTER(BatchStats)]),
     "erosion_matvec": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD]),
     "erosion_matvec_noalloc": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -248,7 +264,10 @@ def far_shapes() -> dict:
     out = {}
     for kind, name in ((0, "fp64"), (1, "fp32")):
         cands = [tuple(desc[12 * kind + 3 * i: 12 * kind + 3 * i + 3]) for i in range(num[kind])]
-        label = lambda c: f"{c[0]}x{c[1]}" + ("-newton" if c[2] else "")
+        if kind == 0:
+            label = lambda c: f"{c[0]}x{c[1]}" + ("-newton" if c[2] else "")
+        else:
+            label = lambda c: f"{c[0]}x{c[1]}-unroll{c[2]}"
         out[name] = {"shape": label(cands[shape[kind]]), "index": shape[kind],
                      "tuned_ms": {label(c): round(ms[8 * kind + i], 4) for i, c in enumerate(cands)}}
     return out

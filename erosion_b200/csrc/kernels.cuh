@@ -225,16 +225,15 @@ __device__ __forceinline__ double rcp_newton(double r2) {
   return r2 > 0.0 ? y : 0.0;
 }
 
+// One CTA's share of the FP64 far field: targets of block bx, tiles of split
+// 'split'.  Shared by k_far64 and the ensemble kernel k_far64_batch.
 template <bool MASK, int NT, int TPT, int RCP>
-__global__ void __launch_bounds__(NT, 512 / NT)
-k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
-        const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
-        double2* __restrict__ partial) {
-  __shared__ double4 sg[FAR_TS];
-  __shared__ double2 sw[FAR_TS];
+__device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __restrict__ ws,
+                                          const int4* __restrict__ tiles, const int* __restrict__ split_ptr,
+                                          const unsigned* __restrict__ mask, int mw, double2* __restrict__ partial,
+                                          int bx, int split, double4* sg, double2* sw) {
   const int N = G.N;
-  const int split = blockIdx.y;
-  const int i0 = blockIdx.x * (NT * TPT) + threadIdx.x;
+  const int i0 = bx * (NT * TPT) + threadIdx.x;
   int it[TPT], cv[TPT];
   double px[TPT], py[TPT], ax[TPT], ay[TPT];
 #pragma unroll
@@ -289,6 +288,16 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
   }
 }
 
+template <bool MASK, int NT, int TPT, int RCP>
+__global__ void __launch_bounds__(NT, 512 / NT)
+k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
+        const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
+        double2* __restrict__ partial) {
+  __shared__ double4 sg[FAR_TS];
+  __shared__ double2 sw[FAR_TS];
+  far64_cta<MASK, NT, TPT, RCP>(G, ws, tiles, split_ptr, mask, mw, partial, blockIdx.x, blockIdx.y, sg, sw);
+}
+
 // ---------------------------------------------------------------------------
 // Far field, FP32 with compensated accumulation (the mixed-precision operator).
 // Same sum as k_far64 but over pairs of DIFFERENT curves only (a target's own
@@ -324,19 +333,18 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t) {
   lo += e;
 }
 
-template <bool MASK, int NT, int TPT>
-__global__ void __launch_bounds__(NT, 512 / NT)
-k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
-        const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
-        const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
-        double2* __restrict__ partial) {
+// One CTA's share of the FP32 far field (targets of block bx, tiles of split
+// 'split'); shared by k_far32 and the ensemble kernel k_far32_batch.
+template <bool MASK, int NT, int TPT, int U>
+__device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* __restrict__ src,
+                                          const float2* __restrict__ tgt, const double2* __restrict__ anchor,
+                                          const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+                                          const int4* __restrict__ tiles, const int* __restrict__ split_ptr,
+                                          const unsigned* __restrict__ mask, int mw, double2* __restrict__ partial,
+                                          int bx, int split, float4* s_pos, float4* s_nrm, float4* s_den) {
   static_assert(TPT % 2 == 0, "targets are processed in lane pairs");
   constexpr int TP = TPT / 2;
-  __shared__ float4 s_pos[F32_TS];
-  __shared__ float4 s_nrm[F32_TS];
-  __shared__ float4 s_den[F32_TS];
-  const int split = blockIdx.y;
-  const int i0 = blockIdx.x * (NT * TPT) + threadIdx.x;
+  const int i0 = bx * (NT * TPT) + threadIdx.x;
   int it[TPT], cv[TPT];
   float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
 #pragma unroll
@@ -370,7 +378,7 @@ k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __
       TX[p] = make_float2(0.f, 0.f);
       TY[p] = make_float2(0.f, 0.f);
     }
-#pragma unroll 2
+#pragma unroll U
     for (int j = 0; j < T.y; ++j) {
       const float4 A = s_pos[j], B = s_nrm[j], C = s_den[j];
       const float2 msx = make_float2(A.x, A.y), msy = make_float2(A.z, A.w);
@@ -405,13 +413,105 @@ k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __
   }
 }
 
+template <bool MASK, int NT, int TPT, int U>
+__global__ void __launch_bounds__(NT, 512 / NT)
+k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
+        const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+        const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
+        double2* __restrict__ partial) {
+  __shared__ float4 s_pos[F32_TS];
+  __shared__ float4 s_nrm[F32_TS];
+  __shared__ float4 s_den[F32_TS];
+  far32_cta<MASK, NT, TPT, U>(N, nout, n, src, tgt, anchor, tile_c, ws32, tiles, split_ptr, mask, mw, partial,
+                           blockIdx.x, blockIdx.y, s_pos, s_nrm, s_den);
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble far field: ONE persistent launch covers the far field of every
+// geometry of an ensemble.  Work item = (geometry, target block, tile split);
+// items are numbered job by job (FarJob*.item0) and CTAs stride over them.
+struct FarJob64 {
+  GeoDev G;
+  const double2* ws;
+  const int4* tiles;
+  const int* split_ptr;
+  const unsigned* mask;   // nullptr: no near masking
+  int mw;
+  double2* partial;
+  int nbx, nsplit;
+  long long item0;
+};
+
+struct FarJob32 {
+  int N, nout, n;
+  const float4* src;
+  const float2* tgt;
+  const double2* anchor;
+  const double2* tile_c;
+  const float2* ws32;
+  const int4* tiles;
+  const int* split_ptr;
+  const unsigned* mask;
+  int mw;
+  double2* partial;
+  int nbx, nsplit;
+  long long item0;
+};
+
+template <class Job>
+__device__ __forceinline__ int find_job(const Job* __restrict__ jobs, int njobs, long long item) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].item0 <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int NT, int TPT, int RCP>
+__global__ void __launch_bounds__(NT, 512 / NT)
+k_far64_batch(const FarJob64* __restrict__ jobs, int njobs, long long nitems) {
+  __shared__ double4 sg[FAR_TS];
+  __shared__ double2 sw[FAR_TS];
+  for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const FarJob64 J = jobs[find_job(jobs, njobs, item)];
+    const int local = (int)(item - J.item0);
+    const int bx = local % J.nbx, q = local / J.nbx;
+    if (J.mask) far64_cta<true, NT, TPT, RCP>(J.G, J.ws, J.tiles, J.split_ptr, J.mask, J.mw, J.partial, bx, q, sg, sw);
+    else far64_cta<false, NT, TPT, RCP>(J.G, J.ws, J.tiles, J.split_ptr, nullptr, 0, J.partial, bx, q, sg, sw);
+    __syncthreads();
+  }
+}
+
+template <int NT, int TPT, int U>
+__global__ void __launch_bounds__(NT, 512 / NT)
+k_far32_batch(const FarJob32* __restrict__ jobs, int njobs, long long nitems) {
+  __shared__ float4 s_pos[F32_TS];
+  __shared__ float4 s_nrm[F32_TS];
+  __shared__ float4 s_den[F32_TS];
+  for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const FarJob32 J = jobs[find_job(jobs, njobs, item)];
+    const int local = (int)(item - J.item0);
+    const int bx = local % J.nbx, q = local / J.nbx;
+    if (J.mask)
+      far32_cta<true, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.ws32, J.tiles, J.split_ptr,
+                               J.mask, J.mw, J.partial, bx, q, s_pos, s_nrm, s_den);
+    else
+      far32_cta<false, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.ws32, J.tiles, J.split_ptr,
+                                nullptr, 0, J.partial, bx, q, s_pos, s_nrm, s_den);
+    __syncthreads();
+  }
+}
+
 // Launch shapes the autotuner chooses from (threads per CTA, targets per
 // thread); solver.cu times each on the geometry at hand.
-// For the FP64 kernel, rcp selects the reciprocal: 0 the division
-// (__drcp_rn), 1 rcp_newton.
+// The third field is a kernel variant: for the FP64 kernel the reciprocal
+// (0 the division __drcp_rn, 1 rcp_newton), for the FP32 kernel the unroll
+// factor of the source loop.
 struct FarShape { int nt, tpt, rcp; };
 constexpr FarShape kFar64Shapes[] = {{256, 2, 0}, {256, 2, 1}, {256, 1, 1}, {128, 4, 1}};
-constexpr FarShape kFar32Shapes[] = {{256, 4, 0}, {256, 8, 0}, {128, 8, 0}, {128, 4, 0}};
+constexpr FarShape kFar32Shapes[] = {{256, 4, 2}, {256, 4, 4}, {128, 4, 4}, {128, 4, 2}};
 constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4;
 
 // Tile centres (middle node) and, per node, the FP32 offset from its tile's
@@ -1206,6 +1306,134 @@ __global__ void k_axpy(double a, const double* __restrict__ x, double* __restric
 __global__ void k_copy(const double* __restrict__ a, double* __restrict__ out, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = a[i];
+}
+
+// ---------------------------------------------------------------------------
+// Arnoldi steps whose column count lives in device memory (*kp), so that one
+// captured CUDA graph serves every iteration of a GMRES cycle.
+
+// out = V[:, *kp + off]
+__global__ void k_col_get(const double* __restrict__ V, long long ldv, const int* __restrict__ kp, int off,
+                          double* __restrict__ out, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = V[(long long)(*kp + off) * ldv + i];
+}
+
+// V[:, *kp + off] = in (times *scale when scale is given)
+__global__ void k_col_put(double* __restrict__ V, long long ldv, const int* __restrict__ kp, int off,
+                          const double* __restrict__ in, const double* __restrict__ scale, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) V[(long long)(*kp + off) * ldv + i] = scale ? in[i] * *scale : in[i];
+}
+
+// part[j][b] = partial dot of columns j < *kp with w over the rows of block b
+__global__ void __launch_bounds__(256)
+k_dot_part_dk(const double* __restrict__ V, long long ldv, const int* __restrict__ kp, const double* __restrict__ w,
+              long long n, int R, double* __restrict__ part) {
+  extern __shared__ double swv[];
+  const int k = *kp;
+  const long long r0 = (long long)blockIdx.x * R;
+  const int rl = (int)max(0LL, min((long long)R, n - r0));
+  for (int t = threadIdx.x; t < rl; t += blockDim.x) swv[t] = w[r0 + t];
+  __syncthreads();
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = wid; j < k; j += nw) {
+    const double* __restrict__ vj = V + (long long)j * ldv + r0;
+    double a = 0.0;
+    for (int t = lane; t < rl; t += 32) a = fma(__ldg(vj + t), swv[t], a);
+    a = warp_sum(a);
+    if (lane == 0) part[(size_t)j * gridDim.x + blockIdx.x] = a;
+  }
+}
+
+// h[j] = sum_b part[j][b] for j < *kp (+ koff); one warp per j, grid-stride.
+__global__ void k_dot_reduce_dk(const double* __restrict__ part, int nb, const int* __restrict__ kp, int koff,
+                                double* __restrict__ h) {
+  const int k = *kp + koff;
+  const int lane = threadIdx.x & 31;
+  for (int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < k; j += gridDim.x * (blockDim.x >> 5)) {
+    double a = 0.0;
+    for (int b = lane; b < nb; b += 32) a += part[(size_t)j * nb + b];
+    a = warp_sum(a);
+    if (lane == 0) h[j] = a;
+  }
+}
+
+// w += sign * V[:, 0:*kp] h
+__global__ void __launch_bounds__(256)
+k_vh_dk(const double* __restrict__ V, long long ldv, const int* __restrict__ kp, const double* __restrict__ h,
+        double sign, double* __restrict__ w, long long n) {
+  __shared__ double sh[1024];
+  const int k = *kp;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  for (int j0 = 0; j0 < k; j0 += 1024) {
+    const int jt = min(1024, k - j0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < jt; t += blockDim.x) sh[t] = h[j0 + t];
+    __syncthreads();
+    if (i < n) {
+      const double* __restrict__ vp = V + (long long)j0 * ldv + i;
+      int j = 0;
+      double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+      for (; j + 3 < jt; j += 4) {
+        a0 = fma(__ldg(vp + (long long)(j)*ldv), sh[j], a0);
+        a1 = fma(__ldg(vp + (long long)(j + 1) * ldv), sh[j + 1], a1);
+        a2 = fma(__ldg(vp + (long long)(j + 2) * ldv), sh[j + 2], a2);
+        a3 = fma(__ldg(vp + (long long)(j + 3) * ldv), sh[j + 3], a3);
+      }
+      for (; j < jt; ++j) a0 = fma(__ldg(vp + (long long)j * ldv), sh[j], a0);
+      acc += (a0 + a1) + (a2 + a3);
+    }
+  }
+  if (i < n) w[i] += sign * acc;
+}
+
+// The Givens step of one Arnoldi iteration on the device (DHEQR,
+// gmres_routines.f:1148, last column).  Column k = *kp of the Hessenberg
+// matrix is h1[0..k-1] + h2[0..k-1] (the two Gram-Schmidt passes) with
+// subdiagonal sqrt(*hn); the previous rotations (cs[2i], cs[2i+1]) are applied,
+// a new rotation zeroes the subdiagonal, the column is stored packed in R
+// (column k-1 at offset (k-1)k/2), prod <- prod * s and rho = |prod r0|.
+// scale <- 1/sqrt(hn) for the next basis vector.  st: 0 running, 2 breakdown
+// (zero diagonal), 3 non-finite.  One thread.
+__global__ void k_givens_step(const int* __restrict__ kp, const double* __restrict__ h1,
+                              const double* __restrict__ h2, const double* __restrict__ hn, double* __restrict__ cs,
+                              double* __restrict__ R, double* __restrict__ prod, const double* __restrict__ r0,
+                              double* __restrict__ rho, double* __restrict__ scale, int* __restrict__ st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int k = *kp;
+  double* col = R + (size_t)(k - 1) * k / 2;
+  const double snormw = sqrt(*hn);
+  bool finite = isfinite(snormw);
+  for (int i = 0; i < k; ++i) {
+    col[i] = h1[i] + h2[i];
+    finite = finite && isfinite(col[i]);
+  }
+  if (!finite) { *st = 3; return; }
+  for (int kk = 0; kk < k - 1; ++kk) {
+    const double c = cs[2 * kk], sn = cs[2 * kk + 1];
+    const double t1 = col[kk], t2 = col[kk + 1];
+    col[kk] = c * t1 - sn * t2;
+    col[kk + 1] = sn * t1 + c * t2;
+  }
+  const double t1 = col[k - 1], t2 = snormw;
+  double c, sn;
+  if (t2 == 0.0) { c = 1.0; sn = 0.0; }
+  else if (fabs(t2) >= fabs(t1)) { const double t = t1 / t2; sn = -1.0 / sqrt(1.0 + t * t); c = -sn * t; }
+  else { const double t = t2 / t1; c = 1.0 / sqrt(1.0 + t * t); sn = -c * t; }
+  cs[2 * (k - 1)] = c;
+  cs[2 * (k - 1) + 1] = sn;
+  col[k - 1] = c * t1 - sn * t2;
+  if (col[k - 1] == 0.0) { *st = 2; return; }
+  *prod *= sn;
+  *rho = fabs(*prod * *r0);
+  *scale = snormw > 0.0 ? 1.0 / snormw : 0.0;
+  *st = 0;
+}
+
+__global__ void k_inc(int* kp) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *kp += 1;
 }
 
 }  // namespace

@@ -247,9 +247,11 @@ static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Sha
               kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 1 && kFar64Shapes[2].rcp == 1 &&
               kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 1,
               "launch_far's FP64 cases");
-static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].nt == 256 &&
-              kFar32Shapes[1].tpt == 8 && kFar32Shapes[2].nt == 128 && kFar32Shapes[2].tpt == 8 &&
-              kFar32Shapes[3].nt == 128 && kFar32Shapes[3].tpt == 4, "launch_far's FP32 cases");
+static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[0].rcp == 2 &&
+              kFar32Shapes[1].nt == 256 && kFar32Shapes[1].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
+              kFar32Shapes[2].nt == 128 && kFar32Shapes[2].tpt == 4 && kFar32Shapes[2].rcp == 4 &&
+              kFar32Shapes[3].nt == 128 && kFar32Shapes[3].tpt == 4 && kFar32Shapes[3].rcp == 2,
+              "launch_far's FP32 cases");
 
 // One far-field launch of the given kind (0 FP64 on wrest, 1 FP32 on ws32)
 // and shape over the tile splits sp[0..nsplit], into out[split * N + i].
@@ -260,13 +262,13 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
   cudaStream_t st = s.st;
   const bool mk = nr.npairs > 0;
   const dim3 g((unsigned)nblk(pr.N, shape_targets(kind, shape)), (unsigned)nsplit);
-#define EB_FAR32(IDX, NT, TPT)                                                                                    \
+#define EB_FAR32(IDX, NT, TPT, U)                                                                                 \
   case IDX:                                                                                                       \
     if (mk)                                                                                                       \
-      k_far32<true, NT, TPT><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p, \
+      k_far32<true, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p, \
                                                s.ws32.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);           \
     else                                                                                                          \
-      k_far32<false, NT, TPT><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,           \
+      k_far32<false, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,           \
                                                 s.tile_c.p, s.ws32.p, s.tiles.p, sp, nullptr, 0, out);    \
     break;
 #define EB_FAR64(IDX, NT, TPT, RCP)                                                                          \
@@ -278,10 +280,10 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
     break;
   if (kind == 1) {
     switch (shape) {
-      EB_FAR32(0, 256, 4)
-      EB_FAR32(1, 256, 8)
-      EB_FAR32(2, 128, 8)
-      EB_FAR32(3, 128, 4)
+      EB_FAR32(0, 256, 4, 2)
+      EB_FAR32(1, 256, 4, 4)
+      EB_FAR32(2, 128, 4, 4)
+      EB_FAR32(3, 128, 4, 2)
       default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
     }
   } else {
@@ -562,36 +564,20 @@ void harvest_far_timing(State& s) {
   }
 }
 
-void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
-  harvest_far_timing(s);
+void operator_prep(State& s, const double* d_den, double* d_vel) {
+  const Problem& pr = s.pr;
+  k_prep<<<pr.M + 1, 256, 0, s.st>>>(s.geo(), d_den, s.ws.p, s.wrest.p, s.ws32.p, d_vel, s.sigdotn.p,
+                                      pr.P.ibary == 1);
+  EB_LAUNCH_CHECK();
+}
+
+int far_slots(const State& s, int prec) { return prec == 1 ? s.nsplit32 + s.nsplitw : s.nsplit64t; }
+
+void operator_post(State& s, const double* d_den, double* d_vel, int nsplit) {
   const Problem& pr = s.pr;
   const GeoDev G = s.geo();
   const Near& nr = s.near;
   cudaStream_t st = s.st;
-  k_prep<<<pr.M + 1, 256, 0, st>>>(G, d_den, s.ws.p, s.wrest.p, s.ws32.p, d_vel, s.sigdotn.p, pr.P.ibary == 1);
-  EB_LAUNCH_CHECK();
-  const int kind = prec == 1 ? 1 : 0;
-  int nsplit = kind ? s.nsplit32 : s.nsplit64t;
-  if (nsplit > 0) {
-    EB_CK(cudaEventRecord(s.ef0, st));
-    launch_far(s, kind, s.far_shape[kind], kind ? s.split_ptr32.p : s.split_ptr64t.p, nsplit, s.partial.p);
-    EB_CK(cudaEventRecord(s.ef1, st));
-    s.far_kind = kind;
-    s.far_pending = true;
-  }
-  if (kind == 1) {
-    // wall sources in FP64, into the partial slots after the FP32 ones
-    EB_CK(cudaEventRecord(s.ew0, st));
-    launch_far(s, 0, s.far_shape[0], s.split_ptrw.p, s.nsplitw, s.partial.p + (size_t)nsplit * pr.N);
-    EB_CK(cudaEventRecord(s.ew1, st));
-    s.farw_pending = true;
-    nsplit += s.nsplitw;
-    s.stats.matvecs_fp32++;
-    if (s.nsplit32 > 0) s.stats.far32_launches++;
-    s.stats.farw_launches++;
-  } else {
-    s.stats.far_launches++;
-  }
   k_self64<<<s.n_self_tasks, 256, 0, st>>>(G, s.ws.p, s.self_tasks.p, s.selfsum.p);
   EB_LAUNCH_CHECK();
   if (nr.npairs > 0) {
@@ -606,6 +592,35 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
                                              nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p,
                                              s.selfsum.p, s.n_self_slots, d_vel);
   EB_LAUNCH_CHECK();
+}
+
+void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
+  harvest_far_timing(s);
+  const Problem& pr = s.pr;
+  cudaStream_t st = s.st;
+  operator_prep(s, d_den, d_vel);
+  const int kind = prec == 1 ? 1 : 0;
+  const int n1 = kind ? s.nsplit32 : s.nsplit64t;
+  if (n1 > 0) {
+    EB_CK(cudaEventRecord(s.ef0, st));
+    launch_far(s, kind, s.far_shape[kind], kind ? s.split_ptr32.p : s.split_ptr64t.p, n1, s.partial.p);
+    EB_CK(cudaEventRecord(s.ef1, st));
+    s.far_kind = kind;
+    s.far_pending = true;
+  }
+  if (kind == 1) {
+    // wall sources in FP64, into the partial slots after the FP32 ones
+    EB_CK(cudaEventRecord(s.ew0, st));
+    launch_far(s, 0, s.far_shape[0], s.split_ptrw.p, s.nsplitw, s.partial.p + (size_t)n1 * pr.N);
+    EB_CK(cudaEventRecord(s.ew1, st));
+    s.farw_pending = true;
+    s.stats.matvecs_fp32++;
+    if (s.nsplit32 > 0) s.stats.far32_launches++;
+    s.stats.farw_launches++;
+  } else {
+    s.stats.far_launches++;
+  }
+  operator_post(s, d_den, d_vel, far_slots(s, prec));
   s.stats.matvecs++;
   s.stats.far32_pairs = s.far32_pairs;
   s.stats.far64_pairs = s.far64_pairs;
@@ -870,6 +885,27 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   }
   *iters = total;
   return EROSION_MAXITER;
+}
+
+// Frees every device buffer a State holds (the next call sets it up again).
+void release_state_buffers(State& s) {
+  DBuf<double>* dbs[] = {&s.dker_body, &s.dker_wall, &s.wx, &s.wy, &s.sp, &s.cur, &s.w, &s.rb, &s.sigdotn,
+                         &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.Z, &s.part, &s.hdev,
+                         &s.ydev, &s.pc_z, &s.pc_u};
+  for (auto* b : dbs) b->release();
+  DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.wrest, &s.partial, &s.bd, &s.pair_out};
+  for (auto* b : d2s) b->release();
+  s.near.src_curve.release(); s.near.pair_tgt.release(); s.near.tptr.release(); s.near.tpairs.release();
+  s.near.bd_off.release(); s.near.bd_work.release(); s.near.bary_work.release(); s.near.mask.release();
+  s.tiles.release(); s.split_ptr.release();
+  s.vcap = 0;
+  s.zcap = 0;
+  s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
+  s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
+  s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();
+  s.split_tune.release(); s.tune_N = -1; s.tuned_shape[0] = s.tuned_shape[1] = -1;
+  s.dker_body_n = s.dker_wall_n = -1;
+  s.geo_valid = false;
 }
 
 }  // namespace eb
@@ -1165,23 +1201,8 @@ int64_t erosion_near_info(int64_t* lw, int64_t* wall_bodies, int64_t* near_pairs
 void erosion_release(void) {
   State& s = state();
   std::lock_guard<std::mutex> lk(s.mu);
-  DBuf<double>* dbs[] = {&s.dker_body, &s.dker_wall, &s.wx, &s.wy, &s.sp, &s.cur, &s.w, &s.rb, &s.sigdotn,
-                         &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.Z, &s.part, &s.hdev,
-                         &s.ydev, &s.pc_z, &s.pc_u};
-  for (auto* b : dbs) b->release();
-  DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.partial, &s.bd, &s.pair_out};
-  for (auto* b : d2s) b->release();
-  s.near.src_curve.release(); s.near.pair_tgt.release(); s.near.tptr.release(); s.near.tpairs.release();
-  s.near.bd_off.release(); s.near.bd_work.release(); s.near.bary_work.release(); s.near.mask.release();
-  s.tiles.release(); s.split_ptr.release();
-  s.vcap = 0;
-  s.zcap = 0;
-  s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
-  s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
-  s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();
-  s.split_tune.release(); s.tune_N = -1; s.tuned_shape[0] = s.tuned_shape[1] = -1;
-  s.dker_body_n = s.dker_wall_n = -1;
-  s.geo_valid = false;
+  release_batch();
+  release_state_buffers(s);
 }
 
 }  // extern "C"

@@ -181,6 +181,7 @@ struct State {
 };
 
 State& state();
+int eb_num_sms();
 void ensure_init(State& s);
 
 // Geometry + near lists + far-field tiles for (xx, yy) already on the device.
@@ -188,6 +189,13 @@ void setup_problem(State& s, const Problem& pr, const double* d_xx, const double
 // vel = A den, device pointers.  prec 0: FP64 far field; 1: FP32 far field
 // between distinct curves + FP64 self-curve sums.
 void apply_operator(State& s, const double* d_den, double* d_vel, int prec = 0);
+// apply_operator in three parts, for callers that batch the far field of
+// several geometries into one launch: k_prep (strengths), then the far field
+// into s.partial (far_slots(s, prec) slots), then the self/near sums and the
+// assembly.
+void operator_prep(State& s, const double* d_den, double* d_vel);
+int far_slots(const State& s, int prec);
+void operator_post(State& s, const double* d_den, double* d_vel, int nsplit);
 void build_rhs(State& s, double* d_rhs);
 // GMRES (SLATEC DGMRES semantics, CGS2 Arnoldi); returns EROSION_* status.
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
@@ -206,6 +214,10 @@ void apply_preconditioner(State& s, const double* v, double* z);
 double device_norm(State& s, const double* d_v, long long n);
 // Adds the last far-field launch's event time to stats.ms_far (after a sync).
 void harvest_far_timing(State& s);
+
+void release_state_buffers(State& s);
+// Frees the ensemble solver's members (batch.cu).
+void release_batch();
 
 // Shear stress / targets (stress.cu)
 void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E);

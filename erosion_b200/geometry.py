@@ -172,6 +172,62 @@ def workload(name: str, seed: int = 0) -> Geometry:
     raise KeyError(name)
 
 
+def superellipse_area(wall) -> float:
+    a, b, p = wall
+    return 4 * a * b * math.gamma(1 + 1 / p) ** 2 / math.gamma(1 + 2 / p)
+
+
+def lattice_pack(M: int, n: int, porosity: float, wall, rng: np.random.Generator, spread: float = 0.15):
+    """M discs whose total area leaves the given porosity inside the wall,
+    with clearance 4 h (h = node spacing 2 pi r / n) between discs and to the
+    wall: radii r_i = rbar (1 + U[-spread, spread]) scaled to the area, centres
+    on random sites of a hexagonal lattice of spacing 2 r_max + 4 h(r_max),
+    jittered within the slack.  The porosity rises (radii shrink) until the
+    lattice has M admissible sites."""
+    area = superellipse_area(wall)
+    rel = 1 + rng.uniform(-spread, spread, M)
+    a, b, _ = wall
+    ring = np.linspace(0, 2 * np.pi, 64, endpoint=False)
+    phi = porosity
+    for _ in range(200):
+        scale = math.sqrt((1 - phi) * area / (math.pi * (rel ** 2).sum()))
+        radii = scale * rel
+        rmax = radii.max()
+        gap = 4 * 2 * math.pi * rmax / n
+        d = 2 * rmax + gap * 1.05
+        xs = np.arange(-a, a + d, d)
+        ys = np.arange(-b, b + d, d * math.sqrt(3) / 2)
+        sites = [(x + (0.5 * d if j % 2 else 0.0), y) for j, y in enumerate(ys) for x in xs]
+        R = rmax + gap
+        ok = [(x, y) for x, y in sites if _inside_wall(x + R * np.cos(ring), y + R * np.sin(ring), wall).all()]
+        if len(ok) >= M:
+            pick = rng.choice(len(ok), M, replace=False)
+            cs = np.array([ok[i] for i in pick])
+            slack = 0.5 * (d - 2 * rmax - gap)
+            cs = cs + rng.uniform(-slack, slack, cs.shape) * 0.5
+            return radii, cs, phi
+        phi = min(0.98, phi + 0.01)
+    raise RuntimeError(f"could not place {M} bodies")
+
+
+def ensemble(count: int, seed: int = 0, bodies=(20, 200), npts=(128, 256, 512), porosity=(0.5, 0.8),
+             nout: int = 2048, wall=CHANNEL_WALL):
+    """An ensemble of independent channel geometries with uneven sizes: body
+    count U{bodies}, nodes per body drawn from npts, porosity U[porosity]
+    (radii scaled to it, lattice_pack), parabolic wall data.  The default is
+    the 64-geometry batching workload when count = 64."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        M = int(rng.integers(bodies[0], bodies[1] + 1))
+        n = int(rng.choice(npts))
+        phi = float(rng.uniform(*porosity))
+        radii, cs, _ = lattice_pack(M, n, phi, wall, rng)
+        xx, yy = make_bodies(n, radii, cs)
+        out.append(Geometry(n, nout, xx, yy, tuple(wall), 0, radii, cs))
+    return out
+
+
 def custom(n: int, nout: int, radii, centers, wall=REFERENCE_WALL, ibc: int = 1) -> Geometry:
     radii = np.asarray(radii, float)
     centers = np.asarray(centers, float).reshape(-1, 2)

@@ -111,3 +111,30 @@ def near_info(M: int):
     npairs = np.zeros(1, np.int64)
     k = L.erosion_near_info(lw.ctypes.data_as(PI64), wb.ctypes.data_as(PI64), npairs.ctypes.data_as(PI64))
     return int(lw[0]), wb[:k].tolist(), int(npairs[0])
+
+
+def solve_batch(geoms, x0=None, allow=(_lib.EROSION_OK,), **kw):
+    """Ensemble solve of independent geometries (one erosion_solve_batch call;
+    all share the parameters, the wall shape and the boundary data of the
+    first).  Returns (list of densities, iterations per geometry, batch stats)."""
+    L = _lib.load()
+    p = params_for(geoms[0], **kw)
+    nb = len(geoms)
+    npts = np.array([g.n for g in geoms], np.int64)
+    nbods = np.array([g.M for g in geoms], np.int64)
+    nout = np.array([g.nout for g in geoms], np.int64)
+    xx = np.ascontiguousarray(np.concatenate([g.xx for g in geoms] + [np.zeros(1)]))
+    yy = np.ascontiguousarray(np.concatenate([g.yy for g in geoms] + [np.zeros(1)]))
+    sizes = [g.ntot for g in geoms]
+    den = np.zeros(sum(sizes)) if x0 is None else np.ascontiguousarray(np.concatenate(x0), dtype=np.float64)
+    nits = np.zeros(nb, np.int64)
+    rc = L.erosion_solve_batch(ctypes.byref(p), nb, npts.ctypes.data_as(PI64), nbods.ctypes.data_as(PI64),
+                               nout.ctypes.data_as(PI64), ptr(xx), ptr(yy), ptr(den), nits.ctypes.data_as(PI64))
+    check(rc, allow)
+    st = _lib.BatchStats()
+    L.erosion_get_batch_stats(ctypes.byref(st))
+    out, o = [], 0
+    for n in sizes:
+        out.append(den[o:o + n].copy())
+        o += n
+    return out, nits, st.as_dict()

@@ -154,6 +154,37 @@ int erosion_solve_device(const erosion_params* p, int64_t npts, int64_t nbods, i
 
 void erosion_get_solve_stats(erosion_solve_stats* s);
 
+/* Ensemble solve (extended API; the reference solves one geometry per call).
+ * nbatch independent geometries, each with its own npts[g], nbods[g],
+ * nouter[g]; xx, yy hold every geometry's body nodes one after another
+ * (npts[g]*nbods[g] each), density every geometry's unknowns one after
+ * another (2*npts*nbods + 3*nbods + 2*nouter each; initial guess in, solution
+ * out), nits[g] receives each geometry's GMRES iterations.  Every geometry is
+ * solved with the method erosion_solve applies for the same parameters (one
+ * erosion_params for all); the geometries advance together, one Arnoldi
+ * iteration per round: the far field of all of them is one persistent launch
+ * per precision and the rest of a round replays one captured CUDA graph.
+ * Returns EROSION_OK or the first non-OK status of a geometry. */
+int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* npts, const int64_t* nbods,
+                        const int64_t* nouter, const double* xx, const double* yy, double* density, int64_t* nits);
+
+typedef struct {
+  int64_t geometries;
+  int64_t rounds;            /* lockstep Arnoldi rounds (graph replays)            */
+  int64_t iterations;        /* GMRES iterations summed over the geometries        */
+  int64_t graph_captures;    /* round graphs captured (pattern or buffer changes)   */
+  double ms_total;           /* device time of the whole ensemble solve            */
+  double pairs64_per_round;  /* FP64 far-field pairs of the last captured round     */
+  double pairs32_per_round;  /* FP32 far-field pairs of the last captured round     */
+  double pairs64_total;      /* FP64 far-field pairs over all rounds               */
+  double pairs32_total;      /* FP32 far-field pairs over all rounds               */
+  double max_true_residual;  /* largest final residual over the geometries         */
+  int64_t shape64, shape32;  /* ensemble launch shapes (indices as erosion_get_far_shapes) */
+  float tune_ms[8];          /* timed candidates: [0..3] FP64, [4..7] FP32 (0 = not timed) */
+} erosion_batch_stats;
+
+void erosion_get_batch_stats(erosion_batch_stats* s);
+
 /* One application of the boundary operator (host arrays) — the reference's
  * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm;
  * precision = 1 applies the mixed-precision operator (FP32 far field from body
@@ -303,8 +334,9 @@ double erosion_peak_tflops(int32_t precision);
 int erosion_set_far_shape(int32_t kind, int32_t shape);
 
 /* The shapes in use: shape[kind] = candidate index; desc[12*kind + 3*i ..] =
- * (threads, targets per thread, reciprocal: 0 division, 1 Newton-Raphson from
- * the FP32 estimate) of candidate i (num_shapes[kind] of them, at most 4,
+ * (threads, targets per thread, variant: for the FP64 kernel the reciprocal,
+ * 0 division or 1 Newton-Raphson from the FP32 estimate; for the FP32 kernel
+ * the unroll factor of the source loop) of candidate i (num_shapes[kind] of them, at most 4,
  * capacity 24 entries); ms[8*kind + i] = the autotuner's time of candidate i
  * in milliseconds (0 when not timed).  Any pointer may be NULL. */
 int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* num_shapes);
