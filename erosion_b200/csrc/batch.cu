@@ -45,14 +45,21 @@ struct Member {
   int sweep = 0, prec = 0, status = EROSION_OK;
   bool in_cycle = false, done = false;
   double true_residual = -1;
+  // the member's stream (its kernels run concurrently with the other
+  // members') and its captured graphs: the part of a round before the far
+  // field, and the part after it for each precision
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_pre = nullptr, ev_post = nullptr;
+  cudaGraphExec_t pre = nullptr, post[2] = {nullptr, nullptr};
+  long long launches_pre = 0, launches_post[2] = {0, 0};
 };
 
 struct Batch {
   std::vector<Member> m;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
   std::vector<int> key;           // per member: -1 idle, else precision of its round
-  long long graph_launch_count = 0;
+  int n64 = 0, n32 = 0;           // far-field jobs of the current key
+  long long items64 = 0, items32 = 0;
+  cudaEvent_t ev_far = nullptr, ev_start = nullptr;
   DBuf<FarJob64> jobs64;
   DBuf<FarJob32> jobs32;
   int shape64 = 1, shape32 = 0;   // indices into kFar64Shapes / kFar32Shapes
@@ -84,11 +91,15 @@ void init_member_state(State& m, const State& lib) {
     if (!*e) EB_CK(cudaEventCreate(e));
 }
 
+void destroy_member_graphs(Member& mb) {
+  if (mb.pre) cudaGraphExecDestroy(mb.pre);
+  for (auto& g : mb.post)
+    if (g) cudaGraphExecDestroy(g);
+  mb.pre = mb.post[0] = mb.post[1] = nullptr;
+}
+
 void destroy_graph(Batch& B) {
-  if (B.exec) cudaGraphExecDestroy(B.exec);
-  if (B.graph) cudaGraphDestroy(B.graph);
-  B.exec = nullptr;
-  B.graph = nullptr;
+  for (auto& mb : B.m) destroy_member_graphs(mb);
   B.key.clear();
 }
 
@@ -296,7 +307,7 @@ bool ensure_capacity(Member& mb) {
   // column kcyc of R
   const long long need_v = mb.kcyc + 2;
   if (need_v > mb.vcap) {
-    long long nc = std::min<long long>(mb.maxl + 1, std::max<long long>(2 * mb.vcap, std::max<long long>(need_v, 64)));
+    long long nc = std::min<long long>(mb.maxl + 1, std::max<long long>(2 * mb.vcap, std::max<long long>(need_v, 128)));
     double* old = s.V.p;
     s.V.grow_keep((size_t)nc * mb.ldv, (size_t)mb.vcap * mb.ldv, st);
     mb.vcap = nc;
@@ -311,14 +322,14 @@ bool ensure_capacity(Member& mb) {
     }
   }
   if (s.pc_active && mb.kcyc + 1 > mb.zcap) {
-    long long nc = std::min<long long>(mb.maxl, std::max<long long>(2 * mb.zcap, std::max<long long>(mb.kcyc + 1, 64)));
+    long long nc = std::min<long long>(mb.maxl, std::max<long long>(2 * mb.zcap, std::max<long long>(mb.kcyc + 1, 128)));
     double* old = s.Z.p;
     s.Z.grow_keep((size_t)nc * mb.ldv, (size_t)mb.zcap * mb.ldv, st);
     mb.zcap = nc;
     moved |= s.Z.p != old;
   }
   if (mb.kcyc + 1 > mb.rcols) {   // packed R (columns 0..kcyc) and the rotations
-    long long nc = std::min<long long>(mb.maxl, std::max<long long>(2 * mb.rcols, std::max<long long>(mb.kcyc + 1, 64)));
+    long long nc = std::min<long long>(mb.maxl, std::max<long long>(2 * mb.rcols, std::max<long long>(mb.kcyc + 1, 128)));
     double* oldR = mb.R.p;
     mb.R.grow_keep((size_t)nc * (nc + 1) / 2, (size_t)mb.rcols * (mb.rcols + 1) / 2, st);
     double* oldc = mb.cs.p;
@@ -326,6 +337,7 @@ bool ensure_capacity(Member& mb) {
     mb.rcols = nc;
     moved |= mb.R.p != oldR || mb.cs.p != oldc;
   }
+  if (moved) destroy_member_graphs(mb);   // they refer to the old buffers
   return moved;
 }
 
@@ -384,36 +396,66 @@ void record_member_post(Member& mb, int prec, double* pinned_slot) {
                         st));
 }
 
-void capture_round(Batch& B, const std::vector<int>& key) {
-  destroy_graph(B);
-  cudaStream_t st = state().st;
-  int n64, n32;
-  long long i64, i32;
-  double p64, p32;
-  build_jobs(B, key, &n64, &i64, &n32, &i32, &p64, &p32);
-  B.stats.pairs64_per_round = p64;
-  B.stats.pairs32_per_round = p32;
+// Captures one member's graphs on its stream (outside any other capture).
+template <class F>
+cudaGraphExec_t capture_on(cudaStream_t st, F&& record, long long* launches) {
   const long long l0 = g_launches;
   EB_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+  cudaGraph_t g = nullptr;
   try {
-    for (size_t i = 0; i < B.m.size(); ++i)
-      if (key[i] >= 0) record_member_pre(B.m[i], (int)i);
-    launch_batch64(B, B.shape64, n64, i64, st);
-    launch_batch32(B, B.shape32, n32, i32, st);
-    for (size_t i = 0; i < B.m.size(); ++i)
-      if (key[i] >= 0) record_member_post(B.m[i], key[i], B.pinned + 2 * i);
+    record();
   } catch (...) {
-    cudaGraph_t g = nullptr;
     cudaStreamEndCapture(st, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
-  EB_CK(cudaStreamEndCapture(st, &B.graph));
-  EB_CK(cudaGraphInstantiate(&B.exec, B.graph, 0));
-  B.graph_launch_count = g_launches - l0;
+  EB_CK(cudaStreamEndCapture(st, &g));
+  cudaGraphExec_t e = nullptr;
+  cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+  cudaGraphDestroy(g);
+  EB_CK(err);
+  *launches = g_launches - l0;
   g_launches = l0;
-  B.key = key;
+  return e;
+}
+
+void capture_member(Batch& B, Member& mb, int idx) {
+  destroy_member_graphs(mb);
+  mb.pre = capture_on(mb.side, [&] { record_member_pre(mb, idx); }, &mb.launches_pre);
+  for (int prec = 0; prec < 2; ++prec)
+    mb.post[prec] = capture_on(mb.side, [&] { record_member_post(mb, prec, B.pinned + 2 * idx); },
+                               &mb.launches_post[prec]);
   B.stats.graph_captures++;
+}
+
+// One round: every active member's pre-graph on its own stream, the
+// ensemble far field on the library stream once they are all done, then the
+// post-graphs, again concurrently.
+void run_round(Batch& B, const std::vector<int>& key) {
+  cudaStream_t st = state().st;
+  EB_CK(cudaEventRecord(B.ev_start, st));
+  for (size_t i = 0; i < B.m.size(); ++i) {
+    if (key[i] < 0) continue;
+    Member& mb = B.m[i];
+    EB_CK(cudaStreamWaitEvent(mb.side, B.ev_start, 0));
+    EB_CK(cudaGraphLaunch(mb.pre, mb.side));
+    g_launches += mb.launches_pre;
+    EB_CK(cudaEventRecord(mb.ev_pre, mb.side));
+    EB_CK(cudaStreamWaitEvent(st, mb.ev_pre, 0));
+  }
+  launch_batch64(B, B.shape64, B.n64, B.items64, st);
+  launch_batch32(B, B.shape32, B.n32, B.items32, st);
+  EB_CK(cudaEventRecord(B.ev_far, st));
+  for (size_t i = 0; i < B.m.size(); ++i) {
+    if (key[i] < 0) continue;
+    Member& mb = B.m[i];
+    EB_CK(cudaStreamWaitEvent(mb.side, B.ev_far, 0));
+    EB_CK(cudaGraphLaunch(mb.post[key[i]], mb.side));
+    g_launches += mb.launches_post[key[i]];
+    EB_CK(cudaEventRecord(mb.ev_post, mb.side));
+    EB_CK(cudaStreamWaitEvent(st, mb.ev_post, 0));
+  }
+  EB_CK(cudaStreamSynchronize(st));
 }
 
 // ---- cycles ------------------------------------------------------------------
@@ -509,12 +551,18 @@ void release_batch() {
   Batch& B = batch();
   destroy_graph(B);
   for (auto& mb : B.m) {
+    if (mb.side) cudaStreamSynchronize(mb.side);
     release_state_buffers(*mb.s);
     DBuf<double>* bufs[] = {&mb.x, &mb.b, &mb.r, &mb.cur, &mb.zc, &mb.out, &mb.h1, &mb.h2, &mb.hn,
                             &mb.cs, &mb.R, &mb.part, &mb.scal, &mb.y};
     for (auto* q : bufs) q->release();
     mb.kdev.release();
     mb.stdev.release();
+    if (mb.ev_pre) cudaEventDestroy(mb.ev_pre);
+    if (mb.ev_post) cudaEventDestroy(mb.ev_post);
+    if (mb.side) cudaStreamDestroy(mb.side);
+    mb.ev_pre = mb.ev_post = nullptr;
+    mb.side = nullptr;
   }
   B.m.clear();
   B.jobs64.release();
@@ -560,6 +608,10 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       mb.s = std::make_unique<State>();
       State& s = *mb.s;
       init_member_state(s, lib);
+      EB_CK(cudaStreamCreateWithFlags(&mb.side, cudaStreamNonBlocking));
+      EB_CK(cudaEventCreateWithFlags(&mb.ev_pre, cudaEventDisableTiming));
+      EB_CK(cudaEventCreateWithFlags(&mb.ev_post, cudaEventDisableTiming));
+      s.st = mb.side;
       Problem pr;
       pr.P = P;
       if (npts[g] < 0 || nbods[g] < 0 || nouter[g] < 0) throw Error(EROSION_BAD_INPUT, "negative sizes");
@@ -567,8 +619,8 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       const size_t nb = (size_t)pr.n * pr.M;
       double* dx = s.d_xx.ensure(std::max<size_t>(nb, 1));
       double* dy = s.d_yy.ensure(std::max<size_t>(nb, 1));
-      h2d(dx, xx + node_off, nb, st);
-      h2d(dy, yy + node_off, nb, st);
+      h2d(dx, xx + node_off, nb, s.st);
+      h2d(dy, yy + node_off, nb, s.st);
       node_off += nb;
       setup_problem(s, pr, dx, dy);
       mb.ntot = s.pr.ntot;
@@ -580,7 +632,7 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       mb.hn.ensure(1); mb.scal.ensure(4); mb.kdev.ensure(1); mb.stdev.ensure(1);
       mb.vcap = mb.zcap = mb.rcols = mb.partcap = 0;
       s.V.release(); s.Z.release();
-      h2d(mb.x.p, density + den_off, (size_t)mb.ntot, st);
+      h2d(mb.x.p, density + den_off, (size_t)mb.ntot, s.st);
       bool zero = true;
       for (long long i = 0; i < mb.ntot && zero; ++i) zero = density[den_off + i] == 0.0;
       den_off += mb.ntot;
@@ -590,15 +642,20 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       mb.abs_tol = P.tol * mb.bnrm;
       mb.relax_abs = P.precision == 1 ? (P.relax_tol > 0 ? P.relax_tol : P.tol * kBatchRelaxFactor) * mb.bnrm : 0.0;
       if (zero) {
-        k_copy<<<nblk(mb.ntot, 256), 256, 0, st>>>(mb.b.p, mb.r.p, mb.ntot);
+        k_copy<<<nblk(mb.ntot, 256), 256, 0, s.st>>>(mb.b.p, mb.r.p, mb.ntot);
         EB_LAUNCH_CHECK();
       } else {
         apply_operator(s, mb.x.p, mb.r.p, 0);
-        k_bminus<<<nblk(mb.ntot, 256), 256, 0, st>>>(mb.b.p, mb.r.p, mb.ntot);
+        k_bminus<<<nblk(mb.ntot, 256), 256, 0, s.st>>>(mb.b.p, mb.r.p, mb.ntot);
         EB_LAUNCH_CHECK();
       }
       pairs_total += (double)s.far64_pairs;
       if (!start_cycle(mb)) finish_cycle(mb, EROSION_OK, P.tol);
+      EB_CK(cudaStreamSynchronize(s.st));
+    }
+    if (!B.ev_far) {
+      EB_CK(cudaEventCreateWithFlags(&B.ev_far, cudaEventDisableTiming));
+      EB_CK(cudaEventCreateWithFlags(&B.ev_start, cudaEventDisableTiming));
     }
     tune_batch(B, pairs_total);
     B.stats.shape64 = B.shape64;
@@ -606,21 +663,25 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
     // lockstep rounds
     std::vector<int> key(nbatch);
     while (true) {
-      bool any = false, moved = false;
+      bool any = false;
       for (int g = 0; g < nbatch; ++g) {
         Member& mb = B.m[g];
         key[g] = -1;
         if (mb.done || !mb.in_cycle) continue;
         mb.prec = (mb.relax_abs > 0.0 && mb.rho < mb.relax_abs) ? 1 : 0;
         key[g] = mb.prec;
-        moved |= ensure_capacity(mb);
+        if (ensure_capacity(mb) || !mb.pre) capture_member(B, mb, g);
         any = true;
       }
       if (!any) break;
-      if (moved || key != B.key || !B.exec) capture_round(B, key);
-      EB_CK(cudaGraphLaunch(B.exec, st));
-      EB_CK(cudaStreamSynchronize(st));
-      g_launches += B.graph_launch_count;
+      if (key != B.key) {
+        double p64, p32;
+        build_jobs(B, key, &B.n64, &B.items64, &B.n32, &B.items32, &p64, &p32);
+        B.stats.pairs64_per_round = p64;
+        B.stats.pairs32_per_round = p32;
+        B.key = key;
+      }
+      run_round(B, key);
       B.stats.rounds++;
       B.stats.pairs64_total += B.stats.pairs64_per_round;
       B.stats.pairs32_total += B.stats.pairs32_per_round;
