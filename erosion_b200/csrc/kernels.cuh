@@ -536,18 +536,21 @@ __global__ void k_geom32(int ntile, const int4* __restrict__ tiles, const double
 
 // FP64 pairs within each curve (i != j), with the full density: the
 // self-interaction part of the far-field sum.  Task = (first target, count
-// <= 256, curve, source chunk); a curve longer than SELF_CHUNK is split into
-// chunks whose partial sums land in separate slots (out[slot*N + i]) and are
-// added in a fixed order by k_combine.
+// <= 256, curve, source chunk); the wall's sources are split into chunks of
+// SELF_CHUNK and a body's into chunks of body_chunk, whose partial sums land in
+// separate slots (out[slot*N + i]) added in a fixed order by k_combine.
 constexpr int SELF_CHUNK = 512;
+constexpr int SELF_CHUNK_BODY = 64;
 __global__ void __launch_bounds__(256)
-k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tasks, double2* __restrict__ out) {
+k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tasks, double2* __restrict__ out,
+         int body_chunk) {
   __shared__ double4 sg[256];
   __shared__ double2 sw[256];
   const int4 tk = tasks[blockIdx.x];   // target start, count, curve, chunk
   const int c = tk.z, chunk = tk.w;
   const int start = curve_start(G, c), len = curve_len(G, c);
-  const int kb = chunk * SELF_CHUNK, ke = min(len, kb + SELF_CHUNK);
+  const int csz = c == 0 ? SELF_CHUNK : body_chunk;
+  const int kb = chunk * csz, ke = min(len, kb + csz);
   const int i = tk.x + threadIdx.x;
   const bool act = threadIdx.x < tk.y;
   const int ic = act ? i : tk.x;
@@ -1123,46 +1126,41 @@ k_bary_list(GeoDev G, const int4* __restrict__ work, const int* __restrict__ src
 // barycentric pairs (in a fixed order per target), the diagonal curvature
 // limit and jump (:937-951, :964-985), stokeslets and rotlets of every body
 // (:992-1049) and the wall's rank-one term (:1115-1118).
+// COMBINE_G consecutive threads share one node: they split the partial-sum
+// slots, the near pairs and the bodies of the stokeslet/rotlet sum, and their
+// sums meet by warp shuffles (launch nblk(N * COMBINE_G, 256) CTAs of 256).
 constexpr int SR_CHUNK = 256;
+constexpr int COMBINE_G = 4;
 __global__ void __launch_bounds__(256)
 k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ partial, int nsplit,
           const int* __restrict__ tptr, const int* __restrict__ tpairs, const double2* __restrict__ pair_out,
-          const double* __restrict__ sigdotn, const double2* __restrict__ selfp, int nself,
+          const double* __restrict__ sigdotn, const double2* __restrict__ selfp, int nself, int nself_body,
           double* __restrict__ vel) {
   __shared__ double4 sc[SR_CHUNK];   // cx, cy, stokeslet x, stokeslet y
   __shared__ double sr[SR_CHUNK];    // rotlet
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = (int)(tid / COMBINE_G), sub = (int)(tid % COMBINE_G);
   const bool act = g < G.N;
   const int gc = act ? g : G.N - 1;
   const double2 p = G.xy[gc];
   double ux = 0.0, uy = 0.0;
-  for (int q = 0; q < nsplit; ++q) {
+  for (int q = sub; q < nsplit; q += COMBINE_G) {
     double2 v = partial[(size_t)q * G.N + gc];
     ux += v.x; uy += v.y;
   }
   if (selfp) {
-    const int ns = gc < G.nout ? nself : 1;   // only the wall is chunked
-    for (int q = 0; q < ns; ++q) {
+    const int ns = gc < G.nout ? nself : nself_body;
+    for (int q = sub; q < ns; q += COMBINE_G) {
       double2 v = selfp[(size_t)q * G.N + gc];
       ux += v.x; uy += v.y;
     }
   }
   if (tptr) {
-    for (int e = tptr[gc]; e < tptr[gc + 1]; ++e) {
+    for (int e = tptr[gc] + sub; e < tptr[gc + 1]; e += COMBINE_G) {
       double2 v = pair_out[tpairs[e]];
       ux += v.x; uy += v.y;
     }
   }
-  const long long ixg = ix_of(G, gc), iyg = iy_of(G, gc);
-  const double sx = den[ixg], sy = den[iyg];
-  const double2 nn = G.nrm[gc];
-  const double cu = G.cur[gc], s = G.sp[gc];
-  const int nc = gc < G.nout ? G.nout : G.n;
-  const double tdd = nn.y * sx - nn.x * sy;
-  ux = ux - cu * tdd * nn.y * s / nc;
-  uy = uy + cu * tdd * nn.x * s / nc;
-  ux -= 0.5 * sx;
-  uy -= 0.5 * sy;
   for (int b0 = 0; b0 < G.M; b0 += SR_CHUNK) {
     __syncthreads();
     for (int t = threadIdx.x; t < SR_CHUNK; t += blockDim.x) {
@@ -1175,7 +1173,7 @@ k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ 
     }
     __syncthreads();
     const int bt = min(SR_CHUNK, G.M - b0);
-    for (int t = 0; t < bt; ++t) {
+    for (int t = sub; t < bt; t += COMBINE_G) {
       const double4 q = sc[t];
       const double rot = sr[t];
       const double rx = p.x - q.x, ry = p.y - q.y;
@@ -1187,12 +1185,29 @@ k_combine(GeoDev G, const double* __restrict__ den, const double2* __restrict__ 
       uy += 0.5 / EB_TWOPI * (-0.5 * lg * q.w + rd * ir * ry) - rot * rx * ir;
     }
   }
+#pragma unroll
+  for (int o = 1; o < COMBINE_G; o <<= 1) {
+    ux += __shfl_xor_sync(0xffffffffu, ux, o);
+    uy += __shfl_xor_sync(0xffffffffu, uy, o);
+  }
+  if (!act || sub != 0) return;
+  const long long ixg = ix_of(G, gc), iyg = iy_of(G, gc);
+  const double sx = den[ixg], sy = den[iyg];
+  const double2 nn = G.nrm[gc];
+  const double cu = G.cur[gc], s = G.sp[gc];
+  const int nc = gc < G.nout ? G.nout : G.n;
+  const double tdd = nn.y * sx - nn.x * sy;
+  ux = ux - cu * tdd * nn.y * s / nc;
+  uy = uy + cu * tdd * nn.x * s / nc;
+  ux -= 0.5 * sx;
+  uy -= 0.5 * sy;
   if (gc < G.nout) {
     const double sg = *sigdotn;
     ux += sg * nn.x;
     uy += sg * nn.y;
   }
-  if (act) { vel[ixg] = ux; vel[iyg] = uy; }
+  vel[ixg] = ux;
+  vel[iyg] = uy;
 }
 
 // Right-hand side of bd_condition (:208-314).
@@ -1220,23 +1235,56 @@ __global__ void k_rhs(GeoDev G, int ibc, int mode, double wall_b, double* __rest
 // ---------------------------------------------------------------------------
 // Krylov kernels (tall-skinny products with the basis V, row-major by vector).
 
-// part[j*gridDim.x + blk] = sum over this CTA's rows of V[j] . w
-__global__ void __launch_bounds__(256)
-k_dot_part(const double* __restrict__ V, long long ldv, int k, const double* __restrict__ w, long long n,
-           int R, double* __restrict__ part) {
-  extern __shared__ double swv[];
+// part[j*gridDim.x + blk] = sum over this CTA's rows of V[j] . w, for j < k.
+// A warp takes four columns at a time (four independent load streams); each
+// column's sum runs in the same order as one column at a time would.
+__device__ __forceinline__ void dot_cols_cta(const double* __restrict__ V, long long ldv, int k,
+                                             const double* __restrict__ w, long long n, int R,
+                                             double* __restrict__ part, double* swv) {
   const long long r0 = (long long)blockIdx.x * R;
   const int rl = (int)max(0LL, min((long long)R, n - r0));
   for (int t = threadIdx.x; t < rl; t += blockDim.x) swv[t] = w[r0 + t];
   __syncthreads();
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = wid; j < k; j += nw) {
-    const double* __restrict__ vj = V + (long long)j * ldv + r0;
-    double s = 0.0;
-    for (int t = lane; t < rl; t += 32) s = fma(__ldg(vj + t), swv[t], s);
-    s = warp_sum(s);
-    if (lane == 0) part[(size_t)j * gridDim.x + blockIdx.x] = s;
+  for (int j0 = 4 * wid; j0 < k; j0 += 4 * nw) {
+    const int jn = min(4, k - j0);
+    const double* __restrict__ v0 = V + (long long)j0 * ldv + r0;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    if (jn == 4) {
+      for (int t = lane; t < rl; t += 32) {
+        const double wt = swv[t];
+        s0 = fma(__ldg(v0 + t), wt, s0);
+        s1 = fma(__ldg(v0 + ldv + t), wt, s1);
+        s2 = fma(__ldg(v0 + 2 * ldv + t), wt, s2);
+        s3 = fma(__ldg(v0 + 3 * ldv + t), wt, s3);
+      }
+    } else {
+      for (int t = lane; t < rl; t += 32) {
+        const double wt = swv[t];
+        s0 = fma(__ldg(v0 + t), wt, s0);
+        if (jn > 1) s1 = fma(__ldg(v0 + ldv + t), wt, s1);
+        if (jn > 2) s2 = fma(__ldg(v0 + 2 * ldv + t), wt, s2);
+      }
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    s3 = warp_sum(s3);
+    if (lane == 0) {
+      double* pj = part + (size_t)j0 * gridDim.x + blockIdx.x;
+      pj[0] = s0;
+      if (jn > 1) pj[gridDim.x] = s1;
+      if (jn > 2) pj[2 * (size_t)gridDim.x] = s2;
+      if (jn > 3) pj[3 * (size_t)gridDim.x] = s3;
+    }
   }
+}
+
+__global__ void __launch_bounds__(256)
+k_dot_part(const double* __restrict__ V, long long ldv, int k, const double* __restrict__ w, long long n,
+           int R, double* __restrict__ part) {
+  extern __shared__ double swv[];
+  dot_cols_cta(V, ldv, k, w, n, R, part, swv);
 }
 
 // h[j] (+)= sum_b part[j][b]; one warp per j.
@@ -1265,15 +1313,19 @@ k_vh(const double* __restrict__ V, long long ldv, int k, const double* __restric
     if (i < n) {
       const double* __restrict__ vp = V + (long long)j0 * ldv + i;
       int j = 0;
-      double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-      for (; j + 3 < jt; j += 4) {
+      double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0;
+      for (; j + 7 < jt; j += 8) {   // eight independent loads in flight
         a0 = fma(__ldg(vp + (long long)(j)*ldv), sh[j], a0);
         a1 = fma(__ldg(vp + (long long)(j + 1) * ldv), sh[j + 1], a1);
         a2 = fma(__ldg(vp + (long long)(j + 2) * ldv), sh[j + 2], a2);
         a3 = fma(__ldg(vp + (long long)(j + 3) * ldv), sh[j + 3], a3);
+        a4 = fma(__ldg(vp + (long long)(j + 4) * ldv), sh[j + 4], a4);
+        a5 = fma(__ldg(vp + (long long)(j + 5) * ldv), sh[j + 5], a5);
+        a6 = fma(__ldg(vp + (long long)(j + 6) * ldv), sh[j + 6], a6);
+        a7 = fma(__ldg(vp + (long long)(j + 7) * ldv), sh[j + 7], a7);
       }
       for (; j < jt; ++j) a0 = fma(__ldg(vp + (long long)j * ldv), sh[j], a0);
-      acc += (a0 + a1) + (a2 + a3);
+      acc += ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
     }
   }
   if (i < n) w[i] += sign * acc;
@@ -1331,19 +1383,7 @@ __global__ void __launch_bounds__(256)
 k_dot_part_dk(const double* __restrict__ V, long long ldv, const int* __restrict__ kp, const double* __restrict__ w,
               long long n, int R, double* __restrict__ part) {
   extern __shared__ double swv[];
-  const int k = *kp;
-  const long long r0 = (long long)blockIdx.x * R;
-  const int rl = (int)max(0LL, min((long long)R, n - r0));
-  for (int t = threadIdx.x; t < rl; t += blockDim.x) swv[t] = w[r0 + t];
-  __syncthreads();
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = wid; j < k; j += nw) {
-    const double* __restrict__ vj = V + (long long)j * ldv + r0;
-    double a = 0.0;
-    for (int t = lane; t < rl; t += 32) a = fma(__ldg(vj + t), swv[t], a);
-    a = warp_sum(a);
-    if (lane == 0) part[(size_t)j * gridDim.x + blockIdx.x] = a;
-  }
+  dot_cols_cta(V, ldv, *kp, w, n, R, part, swv);
 }
 
 // h[j] = sum_b part[j][b] for j < *kp (+ koff); one warp per j, grid-stride.
@@ -1375,15 +1415,19 @@ k_vh_dk(const double* __restrict__ V, long long ldv, const int* __restrict__ kp,
     if (i < n) {
       const double* __restrict__ vp = V + (long long)j0 * ldv + i;
       int j = 0;
-      double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-      for (; j + 3 < jt; j += 4) {
+      double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0;
+      for (; j + 7 < jt; j += 8) {   // eight independent loads in flight
         a0 = fma(__ldg(vp + (long long)(j)*ldv), sh[j], a0);
         a1 = fma(__ldg(vp + (long long)(j + 1) * ldv), sh[j + 1], a1);
         a2 = fma(__ldg(vp + (long long)(j + 2) * ldv), sh[j + 2], a2);
         a3 = fma(__ldg(vp + (long long)(j + 3) * ldv), sh[j + 3], a3);
+        a4 = fma(__ldg(vp + (long long)(j + 4) * ldv), sh[j + 4], a4);
+        a5 = fma(__ldg(vp + (long long)(j + 5) * ldv), sh[j + 5], a5);
+        a6 = fma(__ldg(vp + (long long)(j + 6) * ldv), sh[j + 6], a6);
+        a7 = fma(__ldg(vp + (long long)(j + 7) * ldv), sh[j + 7], a7);
       }
       for (; j < jt; ++j) a0 = fma(__ldg(vp + (long long)j * ldv), sh[j], a0);
-      acc += (a0 + a1) + (a2 + a3);
+      acc += ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
     }
   }
   if (i < n) w[i] += sign * acc;

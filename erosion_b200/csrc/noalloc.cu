@@ -228,10 +228,10 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
     k_far64<false, FAR_NT, FAR_TPT, 0><<<dim3((unsigned)TB, (unsigned)nsplit), FAR_NT, 0, st>>>(
         G, wrest, tiles, split_ptr, nullptr, 0, partial);
     EB_LAUNCH_CHECK();
-    k_self64<<<ntask, 256, 0, st>>>(G, ws, tasks, selfsum);
+    k_self64<<<ntask, 256, 0, st>>>(G, ws, tasks, selfsum, n);   // one chunk per body
     EB_LAUNCH_CHECK();
-    k_combine<<<nblk(N, 256), 256, 0, st>>>(G, d_den, partial, nsplit, nullptr, nullptr, nullptr, sigdotn, selfsum,
-                                            nslots, d_vel);
+    k_combine<<<nblk((long long)N * COMBINE_G, 256), 256, 0, st>>>(G, d_den, partial, nsplit, nullptr, nullptr, nullptr, sigdotn, selfsum,
+                                            nslots, 1, d_vel);
     EB_LAUNCH_CHECK();
     State& s = state();
     std::lock_guard<std::mutex> lk(s.mu);

@@ -209,11 +209,14 @@ static void build_tiles(State& s) {
   // self-curve tasks: (first target, count <= 256, curve, source chunk)
   std::vector<int4> st;
   s.n_self_slots = 1;
+  s.n_self_wall = s.n_self_body = 1;
   for (int c = 0; c <= pr.M; ++c) {
     int start = c == 0 ? 0 : pr.nout + (c - 1) * pr.n, len = c == 0 ? pr.nout : pr.n;
-    int nch = (len + SELF_CHUNK - 1) / SELF_CHUNK;
-    if (c > 0) nch = 1;   // a body's self sum is short; only the wall is chunked
-    if (c == 0) s.n_self_slots = nch;
+    const int csz = c == 0 ? SELF_CHUNK : SELF_CHUNK_BODY;
+    int nch = (len + csz - 1) / csz;
+    if (c == 0) s.n_self_wall = nch;
+    else s.n_self_body = nch;
+    s.n_self_slots = std::max(s.n_self_slots, nch);
     for (int ch = 0; ch < nch; ++ch)
       for (int o = 0; o < len; o += 256) st.push_back(make_int4(start + o, std::min(256, len - o), c, ch));
   }
@@ -578,7 +581,7 @@ void operator_post(State& s, const double* d_den, double* d_vel, int nsplit) {
   const GeoDev G = s.geo();
   const Near& nr = s.near;
   cudaStream_t st = s.st;
-  k_self64<<<s.n_self_tasks, 256, 0, st>>>(G, s.ws.p, s.self_tasks.p, s.selfsum.p);
+  k_self64<<<s.n_self_tasks, 256, 0, st>>>(G, s.ws.p, s.self_tasks.p, s.selfsum.p, SELF_CHUNK_BODY);
   EB_LAUNCH_CHECK();
   if (nr.npairs > 0) {
     k_bdval<<<nr.n_bd_work, BD_NT, 0, st>>>(G, d_den, nr.bd_work.p, nr.src_curve.p, nr.bd_off.p, s.dker_wall.p,
@@ -588,9 +591,9 @@ void operator_post(State& s, const double* d_den, double* d_vel, int nsplit) {
                                                     nr.pair_tgt.p, s.xy.p, s.pair_out.p);
     EB_LAUNCH_CHECK();
   }
-  k_combine<<<nblk(pr.N, 256), 256, 0, st>>>(G, d_den, s.partial.p, nsplit, nr.npairs ? nr.tptr.p : nullptr,
+  k_combine<<<nblk((long long)pr.N * COMBINE_G, 256), 256, 0, st>>>(G, d_den, s.partial.p, nsplit, nr.npairs ? nr.tptr.p : nullptr,
                                              nr.npairs ? nr.tpairs.p : nullptr, s.pair_out.p, s.sigdotn.p,
-                                             s.selfsum.p, s.n_self_slots, d_vel);
+                                             s.selfsum.p, s.n_self_wall, s.n_self_body, d_vel);
   EB_LAUNCH_CHECK();
 }
 

@@ -141,7 +141,7 @@ struct State {
   DBuf<float2> ws32, tgt32;
   DBuf<double2> tile_c, anchor;
   DBuf<int4> self_tasks;
-  int n_self_tasks = 0, n_self_slots = 1;
+  int n_self_tasks = 0, n_self_slots = 1, n_self_wall = 1, n_self_body = 1;
   int pc_wsplit = 1;        // wall-tile splits of the preconditioner's coupling sum
   DBuf<double2> selfsum;
   long long far32_pairs = 0;
