@@ -134,6 +134,9 @@ class Clocks:
 
 # ---------------------------------------------------------------------------
 def dist_setup(args):
+    """One process per GPU (torchrun): NCCL with a GPU, gloo without one (the
+    reference arm and the CPU tests).  The timeout is short so that ranks
+    waiting for a failed one end with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -142,10 +145,23 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=1800))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
+
+
+def max_over_ranks(x: float, dist, local: int = 0) -> float:
+    """The maximum of x over the ranks (x itself on one process)."""
+    if not dist:
+        return x
+    import torch
+    dev = torch.device("cuda", local) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_rate(g, iters_per_step: float, budget_s: float, threads: int | None = None):
@@ -250,11 +266,7 @@ def run_ensemble(args, world, rank, local, dist):
             _, nits, st = stokes.solve_batch(E, **kw)
             stats.append(st)
     torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=torch.device("cuda", local))
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist, local)
     dev_ms = float(np.mean([s["ms_total"] for s in stats]))
     t1 = time.perf_counter()
     seq_dev = 0.0
@@ -300,6 +312,8 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "c4":
         run_ensemble(args, world, rank, local, dist)
+        if dist:
+            dist.destroy_process_group()
         return
     dev = torch.device("cuda", local)
 
@@ -366,10 +380,7 @@ def main():
     ms = ev0.elapsed_time(ev1)
     launches = L.erosion_launch_count() - launches0
     s1 = solve_stats()
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, local)
     value = world * args.steps / (ms * 1e-3)
 
     # roofline of the dominant far-field kernel: FP64 (k_far64) or FP32
@@ -446,11 +457,7 @@ def main():
                 d2h += (int(Mh[0]) * n + 3 * int(Mh[0])) * 8
             e1.record(stream)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e0.elapsed_time(e1), dist, local)
         e2e = {"value": world * args.e2e_steps / (ems * 1e-3), "unit": "steps/s",
                "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
                "entry_point": "erosion_rk2_step (host arrays)"}
