@@ -63,3 +63,32 @@ def test_single_geometry_batch(lib):
     ref, kref, _ = stokes.solve(g, tol=1e-12)
     assert rel(dens[0], ref) < 1e-10
     assert abs(int(nits[0]) - kref) <= 2
+
+
+def test_batch_with_an_empty_channel_and_uneven_walls(lib):
+    empty = G.custom(64, 256, [], [], wall=G.CHANNEL_WALL, ibc=0)
+    ens = [G.ensemble(1, seed=21, bodies=(3, 3), npts=(64,), porosity=(0.9, 0.9), nout=512)[0], empty]
+    dens, nits, st = stokes.solve_batch(ens, tol=1e-12, precond=1)
+    for g, d in zip(ens, dens):
+        ref, _, _ = stokes.solve(g, tol=1e-12, precond=1)
+        assert rel(d, ref) < 1e-10
+
+
+def test_batch_reports_bad_input_and_stays_usable(lib):
+    from erosion_b200 import _lib
+    good = G.ensemble(1, seed=31, bodies=(2, 2), npts=(64,), porosity=(0.9, 0.9), nout=256)[0]
+    bad = G.Geometry(63, 256, good.xx[:63 * 2].copy(), good.yy[:63 * 2].copy(), good.wall, good.ibc,
+                     good.radii, good.centers)
+    with pytest.raises(_lib.ErosionError) as e:
+        stokes.solve_batch([good, bad], tol=1e-10)
+    assert e.value.code == _lib.EROSION_BAD_INPUT
+    dens, nits, _ = stokes.solve_batch([good], tol=1e-10)
+    assert nits[0] > 0 and np.isfinite(dens[0]).all()
+
+
+def test_batch_iteration_cap(lib, ens):
+    from erosion_b200 import _lib
+    dens, nits, st = stokes.solve_batch(ens, tol=1e-14, maxl=5, precond=1,
+                                        allow=(_lib.EROSION_OK, _lib.EROSION_MAXITER))
+    assert (nits <= 5).all()
+    assert _lib.load().erosion_last_status() == _lib.EROSION_MAXITER
