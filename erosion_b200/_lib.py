@@ -145,6 +145,8 @@ SIGNATURES = {
     "erosion_solve_device": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, PI64]),
     "erosion_get_solve_stats": (None, [POINTER(SolveStats)]),
+    "computepressure_": (None, [PI64, PI64, PI64, PD, PD, PD, PD]),
+    "erosion_pressure": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD]),
     "erosion_solve_batch": (c_int, [POINTER(ErosionParams), c_int32, PI64, PI64, PI64, PD, PD, PD, PI64]),
     "erosion_get_batch_stats": (None, [POINTER(BatchStats)]),
     "erosion_matvec": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD]),

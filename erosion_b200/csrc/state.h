@@ -221,6 +221,8 @@ void release_batch();
 
 // Shear stress / targets (stress.cu)
 void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E);
+// Pressure on the body boundaries (computePressure).
+void body_pressure(State& s, const double* d_den, double* d_p);
 void qoi_targets(State& s, const double* d_den, long long ntar, const double* d_xt, const double* d_yt,
                  double* d_u, double* d_v, double* d_p, double* d_w);
 

@@ -368,12 +368,109 @@ static void bdval_all(State& s, const double* d_den, DBuf<double2>& bd_all) {
 
 int eb_num_sms();
 
+// ---------------------------------------------------------------------------
+// Pressure on the body boundaries (computePressure, stokesSolver.f:4644-4885).
+// Every pair: (2 (r.n)(r.s)/rho^4 - (n.s)/rho^2) w_j with the trapezoid weight
+// w = speed (2pi/n_c)/pi.  Targets: body nodes; sources: every tile, split
+// over blockIdx.y.  A target's own body uses odd-even quadrature: sources of
+// the other index parity only, weight doubled, density minus its value at the
+// target (:4728-4787).
+__global__ void __launch_bounds__(256)
+k_pressure_sum(GeoDev G, const double* __restrict__ den, const int4* __restrict__ tiles,
+               const int* __restrict__ split_ptr, double* __restrict__ part) {
+  __shared__ double4 sg[FAR_TS];
+  __shared__ double2 sd[FAR_TS];
+  __shared__ double sw[FAR_TS];
+  __shared__ int sl[FAR_TS];
+  const int nb = G.n * G.M;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tc = t < nb ? t : nb - 1;
+  const int g = G.nout + tc;
+  const int b = tc / G.n, k = tc - b * G.n, curve = 1 + b;
+  const double2 p = G.xy[g];
+  const double sxk = den[ix_of(G, g)], syk = den[iy_of(G, g)];
+  double acc = 0.0;
+  const int split = blockIdx.y;
+  for (int ti = split_ptr[split]; ti < split_ptr[split + 1]; ++ti) {
+    const int4 T = tiles[ti];
+    __syncthreads();
+    for (int q = threadIdx.x; q < T.y; q += blockDim.x) {
+      const int j = T.x + q;
+      const double2 xy = G.xy[j], nn = G.nrm[j];
+      sg[q] = make_double4(xy.x, xy.y, nn.x, nn.y);
+      sd[q] = make_double2(den[ix_of(G, j)], den[iy_of(G, j)]);
+      sw[q] = G.w[j];
+      sl[q] = j - curve_start(G, T.z);   // index within its curve
+    }
+    __syncthreads();
+    const bool own = T.z == curve;
+    for (int q = 0; q < T.y; ++q) {
+      if (own && ((sl[q] & 1) == (k & 1))) continue;
+      const double4 sq = sg[q];
+      const double2 dq = sd[q];
+      const double sx = own ? dq.x - sxk : dq.x, sy = own ? dq.y - syk : dq.y;
+      const double rx = p.x - sq.x, ry = p.y - sq.y;
+      const double rho2 = rx * rx + ry * ry;
+      const double rdn = rx * sq.z + ry * sq.w, rds = rx * sx + ry * sy, dn = sq.z * sx + sq.w * sy;
+      const double v = (2.0 * rdn * rds / rho2 / rho2 - dn / rho2) * sw[q];
+      acc += own ? 2.0 * v : v;
+    }
+  }
+  if (t < nb) part[(size_t)split * nb + t] = acc;
+}
+
+// Split sums, the jump -(d sigma/ds . tangent) with the spectral derivative
+// (the circulant d[m] of fourierDiff) and the stokeslet pressure
+// (r . lambda)/(2 pi rho^2) of every body (:4829-4881); one thread per node.
+__global__ void __launch_bounds__(256)
+k_pressure_final(GeoDev G, const double* __restrict__ den, const double* __restrict__ part, int nsplit,
+                 const double* __restrict__ dk, double* __restrict__ out) {
+  const int nb = G.n * G.M;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const int b = t / G.n, k = t - b * G.n, g = G.nout + t;
+  double acc = 0.0;
+  for (int q = 0; q < nsplit; ++q) acc += part[(size_t)q * nb + t];
+  double dx = 0.0, dy = 0.0;
+  for (int j = 0; j < G.n; ++j) {
+    int m = k - j;
+    if (m < 0) m += G.n;
+    const double d = __ldg(dk + m);
+    const int gj = G.nout + b * G.n + j;
+    dx = fma(d, den[ix_of(G, gj)], dx);
+    dy = fma(d, den[iy_of(G, gj)], dy);
+  }
+  const double2 nn = G.nrm[g];
+  const double spd = G.sp[g];
+  acc -= (dx / spd) * (-nn.y) + (dy / spd) * nn.x;
+  const double2 p = G.xy[g];
+  for (int s = 0; s < G.M; ++s) {
+    const double2 c = G.cen[s];
+    const double rx = p.x - c.x, ry = p.y - c.y;
+    acc += (rx * den[ic_of(G, s, 0)] + ry * den[ic_of(G, s, 1)]) / (EB_TWOPI * (rx * rx + ry * ry));
+  }
+  out[t] = acc;
+}
+
 static int source_splits(int ntasks, int ncurves, std::vector<int>& sc) {
   int want = std::max(1, (4 * eb_num_sms() + ntasks - 1) / std::max(ntasks, 1));
   int S = std::max(1, std::min(want, ncurves));
   sc.resize(S + 1);
   for (int q = 0; q <= S; ++q) sc[q] = (int)((long long)q * ncurves / S);
   return S;
+}
+
+void body_pressure(State& s, const double* d_den, double* d_p) {
+  const Problem& pr = s.pr;
+  const GeoDev G = s.geo();
+  const int nb = pr.n * pr.M;
+  if (nb == 0) return;
+  static DBuf<double> part;
+  part.ensure((size_t)s.nsplit * nb);
+  k_pressure_sum<<<dim3(nblk(nb, 256), s.nsplit), 256, 0, s.st>>>(G, d_den, s.tiles.p, s.split_ptr.p, part.p);
+  EB_LAUNCH_CHECK();
+  k_pressure_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, part.p, s.nsplit, s.dker_body.p, d_p);
+  EB_LAUNCH_CHECK();
 }
 
 void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E) {
@@ -546,6 +643,27 @@ int erosion_shear_stress_device(const erosion_params* p, int64_t npts, int64_t n
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
   });
+}
+
+int erosion_pressure(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                     const double* yy, const double* density, double* pressure) {
+  return guarded2([&](State& s) {
+    Problem pr = problem_of(p, npts, nbods, nouter);
+    if (pr.M == 0) return EROSION_OK;
+    host_setup(s, pr, xx, yy, density);
+    const size_t nb = (size_t)s.pr.n * s.pr.M;
+    static DBuf<double> dp;
+    dp.ensure(nb);
+    body_pressure(s, s.d_den.p, dp.p);
+    d2h(pressure, dp.p, nb, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    return EROSION_OK;
+  });
+}
+
+void computepressure_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter, const double* xx,
+                      const double* yy, const double* density, double* pressure) {
+  erosion_pressure(nullptr, *npts, *nbods, *nouter, xx, yy, density, pressure);
 }
 
 void computeshearstress_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter, const double* xx,

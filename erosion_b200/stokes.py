@@ -104,6 +104,17 @@ def qoi_targets(g, den, xt, yt, **kw):
     return out
 
 
+def pressure(g, den, **kw):
+    """Pressure on the body boundaries (computepressure_ semantics)."""
+    L = _lib.load()
+    p = params_for(g, **kw)
+    den = np.ascontiguousarray(den, dtype=np.float64)
+    out = np.zeros(g.n * g.M)
+    xx, yy = _xy(g)
+    check(L.erosion_pressure(ctypes.byref(p), g.n, g.M, g.nout, ptr(xx), ptr(yy), ptr(den), ptr(out)))
+    return out
+
+
 def near_info(M: int):
     L = _lib.load()
     lw = np.zeros(1, np.int64)

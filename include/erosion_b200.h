@@ -214,6 +214,19 @@ int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int64_t nbods,
                            const double* d_xx, const double* d_yy, const double* d_den, double* d_vel,
                            void* stream);
 
+/* Pressure on the body boundaries for a given density: replaces
+ * computePressure (stokesSolver.f:4644-4885), which PostProcess.jl:103-113
+ * (compute_pressure) binds as `computepressure_`.  Wall sources and other
+ * bodies by the trapezoid rule, a body's own nodes by odd-even quadrature on
+ * the density less its value at the target, plus the jump and the stokeslet
+ * pressure.  pressure: [npts*nbods]. */
+void computepressure_(const int64_t* npts, const int64_t* nbods, const int64_t* nouter, const double* xx,
+                      const double* yy, const double* density, double* pressure);
+
+/* Same with the extended parameters (wall shape); returns a status. */
+int erosion_pressure(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* xx,
+                     const double* yy, const double* density, double* pressure);
+
 /* The right-hand side of bd_condition (stokesSolver.f:208-314). */
 int erosion_rhs(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                 const double* xx, const double* yy, double* rhs);

@@ -45,6 +45,7 @@ class Oracle:
         L.oracle_geometry.argtypes = [c_int64] * 3 + [PD] * 15
         L.oracle_shear_stress.argtypes = [c_int64] * 3 + [PD, PD, PD, c_int64, PD, PD, PD]
         L.oracle_qoi_targets.argtypes = [c_int64] * 4 + [PD, PD, PD, c_int64, PD, PD, PD, PD, PD, PD, PD]
+        L.oracle_pressure.argtypes = [c_int64] * 3 + [PD, PD, PD, PD, PD]
         L.oracle_near_wall.restype = c_int64
         L.oracle_near_wall.argtypes = [c_int64] * 3 + [PD, PD, PD, PI64, PI64]
         L.oracle_stokes_dlp.argtypes = [c_int64, c_int64, PD, PD, PD, PD, PD, PD, c_int64, PD, PD, c_int64, PD]
@@ -112,6 +113,12 @@ class Oracle:
         self.L.oracle_qoi_targets(g.n, g.M, g.nout, ibary, _p(g.xx), _p(g.yy), _p(den), len(xt), _p(xt), _p(yt),
                                   _p(_wall(g.wall)), *[_p(o) for o in out])
         return out
+
+    def pressure(self, g, den):
+        p = np.zeros(g.n * g.M)
+        den = np.ascontiguousarray(den, dtype=np.float64)
+        self.L.oracle_pressure(g.n, g.M, g.nout, _p(g.xx), _p(g.yy), _p(den), _p(_wall(g.wall)), _p(p))
+        return p
 
     def near_wall(self, g):
         lw = np.zeros(1, np.int64)

@@ -966,6 +966,64 @@ void classify(const Geo& g, int ntar, const double* xt, const double* yt, int* i
   }
 }
 
+// computePressure (stokesSolver.f:4644-4885): the pressure on the body
+// boundaries.  Kernel of every pair: (2 (r.n)(r.s)/rho^4 - (n.s)/rho^2) times
+// the trapezoid weight speed * 2pi/n_c / pi.  Wall sources (:4692-4719) and the
+// other bodies' sources (:4790-4823) by the trapezoid rule; a body's own
+// nodes (:4728-4787) by odd-even quadrature (targets of one parity, sources of
+// the other, weight doubled) applied to the density minus its value at the
+// target; then the jump -(d sigma/ds . tangent) (:4829-4855) and the
+// stokeslet pressure (r . lambda)/(2 pi rho^2) (:4860-4881).
+void body_pressure(const Geo& g, const double* den, double* p) {
+  const int n = g.n, M = g.M, nout = g.nout;
+  auto kern = [](double rx, double ry, double nx, double ny, double sx, double sy) {
+    const double rho2 = rx * rx + ry * ry;
+    const double rdn = rx * nx + ry * ny, rds = rx * sx + ry * sy, dn = nx * sx + ny * sy;
+    return 2.0 * rdn * rds / rho2 / rho2 - dn / rho2;
+  };
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < M * n; ++t) {
+    const int b = t / n, k = t % n;
+    const double xt = g.x[t], yt = g.y[t];
+    double acc = 0.0;
+    for (int j = 0; j < nout; ++j)
+      acc += kern(xt - g.xo[j], yt - g.yo[j], g.px0[j], g.py0[j], den[iwx(g, j)], den[iwy(g, j)]) * g.speed0[j] *
+             TWOPI / nout / PI;
+    const double sxk = den[ibx(g, b, k)], syk = den[iby(g, b, k)];
+    for (int s = 0; s < M; ++s) {
+      for (int j = 0; j < n; ++j) {
+        const int q = s * n + j;
+        const double w = g.speed[q] * TWOPI / n / PI;
+        if (s == b) {
+          if ((j & 1) == (k & 1)) continue;
+          acc += 2.0 * kern(xt - g.x[q], yt - g.y[q], g.px[q], g.py[q], den[ibx(g, s, j)] - sxk,
+                            den[iby(g, s, j)] - syk) * w;
+        } else {
+          acc += kern(xt - g.x[q], yt - g.y[q], g.px[q], g.py[q], den[ibx(g, s, j)], den[iby(g, s, j)]) * w;
+        }
+      }
+    }
+    p[t] = acc;
+  }
+  std::vector<cd> z(n);
+  for (int b = 0; b < M; ++b) {
+    for (int k = 0; k < n; ++k) z[k] = cd(den[ibx(g, b, k)], den[iby(g, b, k)]);
+    fourier_diff(n, z.data());
+    for (int k = 0; k < n; ++k) {
+      const int t = b * n + k;
+      const double tx = -g.py[t], ty = g.px[t];
+      p[t] -= (z[k].real() / g.speed[t]) * tx + (z[k].imag() / g.speed[t]) * ty;
+    }
+  }
+  for (int s = 0; s < M; ++s) {
+    const double l1 = den[ic(g, s, 0)], l2 = den[ic(g, s, 1)];
+    for (int t = 0; t < M * n; ++t) {
+      const double rx = g.x[t] - g.cx[s], ry = g.y[t] - g.cy[s];
+      p[t] += 1.0 / TWOPI * (rx * l1 + ry * l2) / (rx * rx + ry * ry);
+    }
+  }
+}
+
 void qoi_targets(const Geo& g, int ibary, const double* den, int ntar, const double* xt, const double* yt,
                  double* ut, double* vt, double* pt, double* wt) {
   const int nout = g.nout, n = g.n, M = g.M;
@@ -1189,6 +1247,14 @@ void oracle_qoi_targets(int64_t n, int64_t M, int64_t nout, int64_t ibary, const
   Geo g;
   build_geo(g, int(n), int(M), int(nout), xx, yy, wall_from(wallp));
   qoi_targets(g, int(ibary), density, int(ntar), xt, yt, ut, vt, pt, wt);
+}
+
+// computePressure (stokesSolver.f:4644-4885).
+void oracle_pressure(int64_t n, int64_t M, int64_t nout, const double* xx, const double* yy, const double* density,
+                     const double* wallp, double* pressure) {
+  Geo g;
+  build_geo(g, int(n), int(M), int(nout), xx, yy, wall_from(wallp));
+  body_pressure(g, density, pressure);
 }
 
 }  // extern "C"

@@ -51,7 +51,7 @@ def make_operator_fixture(o: Oracle) -> dict:
     xt, yt = qoi_points()
     u, v, p, w = o.qoi_targets(g, den, xt, yt)
     out.update(density=den, nits_tight=nits, nits_1e8=nits8, tau=tau, E=E, tau_trap=tau0, xt=xt, yt=yt,
-               utar=u, vtar=v, ptar=p, vortar=w)
+               utar=u, vtar=v, ptar=p, vortar=w, pressure=o.pressure(g, den))
     return out
 
 

@@ -57,6 +57,7 @@ def test_tight_solve_and_stress_match_golden(lib, fx):
     out = stokes.qoi_targets(g, fx["density"], fx["xt"], fx["yt"])
     for a, k in zip(out, ("utar", "vtar", "ptar", "vortar")):
         assert rel(a, fx[k]) < 1e-9, k
+    assert rel(stokes.pressure(g, fx["density"]), fx["pressure"]) < 1e-10
 
 
 def test_rk2_step_matches_golden(lib):

@@ -87,3 +87,34 @@ def test_pressure_drop_flux_consistency(lib, small):
     up = stokes.qoi_targets(small, den, np.full(13, 2.0), ylocs)[0]
     um = stokes.qoi_targets(small, den, np.full(13, -2.0), ylocs)[0]
     assert abs(up.mean() - um.mean()) / abs(0.5 * (up.mean() + um.mean())) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["ref-small", "c1"])
+def test_boundary_pressure_matches_oracle(lib, oracle, name):
+    g = G.workload(name)
+    den = oracle.solve(g, tol=1e-12)[0]
+    a = stokes.pressure(g, den)
+    b = oracle.pressure(g, den)
+    # the shear stress bound: close bodies (c1 gaps of 0.02) make the 1/rho^4
+    # pairs amplify summation-order rounding to ~1e-10
+    assert np.abs(a - b).max() / np.abs(b).max() < 1e-9
+
+
+def test_computepressure_abi_entry(lib, oracle, small, small_den):
+    import ctypes
+    from erosion_b200 import _lib
+    i64 = lambda v: ctypes.byref(ctypes.c_int64(v))
+    out = np.zeros(small.n * small.M)
+    lib.computepressure_(i64(small.n), i64(small.M), i64(small.nout), _lib.ptr(small.xx), _lib.ptr(small.yy),
+                         _lib.ptr(small_den), _lib.ptr(out))
+    assert lib.erosion_last_status() == 0
+    ref = oracle.pressure(small, small_den)
+    assert np.abs(out - ref).max() / np.abs(ref).max() < 1e-10
+
+
+def test_boundary_pressure_manufactured(lib):
+    r = 0.2
+    g = G.custom(64, 256, [r], [[0.0, 0.0]])
+    den, _, _ = stokes.solve(g, tol=1e-13, rhs_mode=1)
+    exact = (g.xx + 2 * g.yy) / (2 * np.pi * (g.xx ** 2 + g.yy ** 2))
+    assert np.abs(stokes.pressure(g, den) - exact).max() < 1e-9 * np.abs(exact).max()

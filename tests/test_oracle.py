@@ -72,6 +72,7 @@ def test_oracle_reproduces_golden_solve_and_stress(oracle, fx):
     u, v, p, w = oracle.qoi_targets(g, fx["density"], fx["xt"], fx["yt"])
     for a, k in zip((u, v, p, w), ("utar", "vtar", "ptar", "vortar")):
         assert rel(a, fx[k]) < 1e-12, k
+    assert rel(oracle.pressure(g, fx["density"]), fx["pressure"]) < 1e-12
 
 
 def test_oracle_reproduces_golden_rk2_step(oracle):
@@ -99,6 +100,18 @@ def test_manufactured_known_answer(oracle):
     sy = den[2 * nout + n:2 * nout + 2 * n]
     assert np.abs(sx - (1 / r + 3 * g.yy / r ** 3)).max() < 1e-8 * 375
     assert np.abs(sy - (2 / r - 3 * g.xx / r ** 3)).max() < 1e-8 * 375
+
+
+def test_boundary_pressure_of_the_manufactured_solution(oracle):
+    """computePressure (stokesSolver.f:4644-4885) on the manufactured solution
+    of stokesSolver.f:220-257: the rigid-motion density has no exterior double
+    layer, so the boundary pressure is the stokeslet's, (r . lambda)/(2 pi rho^2)
+    with lambda = (1, 2) (the rotlet is pressure-free)."""
+    r = 0.2
+    g = G.custom(64, 256, [r], [[0.0, 0.0]])
+    den, _, _, _ = oracle.solve(g, tol=1e-13, rhs_mode=1)
+    exact = (g.xx + 2 * g.yy) / (2 * np.pi * (g.xx ** 2 + g.yy ** 2))
+    assert np.abs(oracle.pressure(g, den) - exact).max() < 1e-9 * np.abs(exact).max()
 
 
 def test_constant_density_double_layer_identity(oracle):
