@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 
 import numpy as np
 
@@ -226,6 +227,30 @@ def ensemble(count: int, seed: int = 0, bodies=(20, 200), npts=(128, 256, 512), 
         xx, yy = make_bodies(n, radii, cs)
         out.append(Geometry(n, nout, xx, yy, tuple(wall), 0, radii, cs))
     return out
+
+
+_INPUT_GEOS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                           "input_geos.npz")
+
+
+def reference_inputs() -> list[str]:
+    """Names of the reference's simulation input geometries (``01-3`` ...
+    ``80-9``: body count and seed), extracted from its JLD2 files."""
+    with np.load(_INPUT_GEOS) as d:
+        return sorted({k.split("/")[0] for k in d.files})
+
+
+def reference_input(name: str, npts: int = 128, nouter: int = 1024) -> Geometry:
+    """One of the reference's input circle packings as circs2thlenden builds it
+    (Main.jl:37-45 with the ParamSet defaults npts = 128, nouter = 1024, the
+    3 x 1 wall and uniform wall data), from the extracted fixture
+    (tests/golden/make_input_geos.py); erosion_b200.jld2.circles reads the
+    original files directly."""
+    with np.load(_INPUT_GEOS) as d:
+        r, xc, yc = d[f"{name}/rvec"], d[f"{name}/xc"], d[f"{name}/yc"]
+    cs = np.stack([xc, yc], 1)
+    xx, yy = make_bodies(npts, r, cs)
+    return Geometry(npts, nouter, xx, yy, REFERENCE_WALL, 1, np.asarray(r, float), cs)
 
 
 def custom(n: int, nout: int, radii, centers, wall=REFERENCE_WALL, ibc: int = 1) -> Geometry:

@@ -110,6 +110,14 @@ def circs2thlenden(npts: int, rvec, xc, yc) -> ThLenDenType:
     return new_thlenden([circ2thlen(npts, r, x, y) for r, x, y in zip(rvec, xc, yc)])
 
 
+def circs2thlenden_file(params: ParamSet, path: str) -> ThLenDenType:
+    """circs2thlenden(params) of Main.jl:37-45: the initial state from a JLD2
+    circle file (rvec, xc, yc), read with erosion_b200.jld2."""
+    from . import jld2
+    rvec, xc, yc = jld2.circles(path)
+    return circs2thlenden(params.npts, rvec, xc, yc)
+
+
 def pack_state(thlenden: ThLenDenType):
     tl = thlenden.thlenvec
     th = np.ascontiguousarray(np.concatenate([b.theta for b in tl]), dtype=np.float64)

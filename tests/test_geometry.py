@@ -1,6 +1,8 @@
 """The seeded synthetic geometries (CPU): every body node strictly inside the
 wall, the configured clearances between bodies and to the wall, the
 configured sizes, and determinism in the seed."""
+import os
+
 import numpy as np
 import pytest
 
@@ -56,3 +58,23 @@ def test_lattice_pack_reaches_target_porosity():
     radii, cs, phi = G.lattice_pack(60, 256, 0.6, G.CHANNEL_WALL, rng)
     assert phi == pytest.approx(0.6)
     assert np.pi * (radii ** 2).sum() / G.superellipse_area(G.CHANNEL_WALL) == pytest.approx(0.4, rel=1e-9)
+
+
+def test_reference_input_geometries_load():
+    names = G.reference_inputs()
+    assert len(names) == 31 and "02-8" in names and "100-3" in names
+    for name in names:
+        g = G.reference_input(name)
+        assert g.M == int(name.split("-")[0])
+        assert (g.n, g.nout, g.wall) == (128, 1024, G.REFERENCE_WALL)
+        assert inside(g)
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/simulations/input_geos"),
+                    reason="the reference repository is not checked out here")
+def test_jld2_reader_matches_fixture():
+    from erosion_b200 import jld2
+    for name in ("01-3", "20-11", "100-9"):
+        r, xc, yc = jld2.circles(f"/root/reference/simulations/input_geos/{name}.jld2")
+        g = G.reference_input(name)
+        assert np.array_equal(r, g.radii) and np.array_equal(xc, g.centers[:, 0])

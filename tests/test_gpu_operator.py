@@ -115,3 +115,22 @@ def test_manufactured_known_answer(lib):
     x, y = g.xx, g.yy
     assert np.abs(sx - (1 / r + 3 * y / r ** 3)).max() < 1e-8 * 375
     assert np.abs(sy - (2 / r - 3 * x / r ** 3)).max() < 1e-8 * 375
+
+
+def test_reference_input_geometries(lib, oracle):
+    """Geometries the reference's own simulations start from (input_geos,
+    ParamSet defaults): operator parity for the 20-circle packing 20-11 (its
+    unpreconditioned solve needs more than N iterations, so the tight solve
+    is compared on the two-circle 02-8), and the preconditioned mixed solve
+    of 20-11 reaching the FP64 answer."""
+    g = G.reference_input("20-11")
+    den = rand_den(g, 3)
+    assert rel(stokes.matvec(g, den), oracle.matvec(g, den, mode=1)) < MATVEC_RTOL
+    x64, _, _ = stokes.solve(g, tol=1e-11, precond=1)
+    x32, _, st = stokes.solve(g, precision=1, precond=1)
+    assert np.linalg.norm(x32 - x64) / np.linalg.norm(x64) < 1e-6
+    assert st["true_residual"] <= 2e-8
+    g2 = G.reference_input("02-8")
+    a, _, _ = stokes.solve(g2, tol=1e-12)
+    b, _, ierr, _ = oracle.solve(g2, tol=1e-12)
+    assert ierr == 0 and rel(a, b) < 1e-10
