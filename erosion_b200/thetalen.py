@@ -93,6 +93,40 @@ class ThLenDenType:
     denrot: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
 
 
+def save_thldvec(path: str, thldvec: list, params: ParamSet | None = None) -> None:
+    """The run output of Main.jl:130 (`jldsave(outfile; params, thldvec,
+    cpu_hours)`) as a numpy .npz: for every saved state k, the time, each
+    body's theta, L, xsm, ysm, matau, and the density and rotated density
+    when present; the ParamSet fields as scalars."""
+    out = {"nstates": np.array(len(thldvec))}
+    for k, st in enumerate(thldvec):
+        out[f"s{k}/tt"] = np.array(st.tt)
+        out[f"s{k}/theta"] = np.array([b.theta for b in st.thlenvec]) if st.thlenvec else np.zeros((0, 0))
+        for f in ("len", "xsm", "ysm", "matau"):
+            out[f"s{k}/{f}"] = np.array([getattr(b, f) for b in st.thlenvec], float)
+        out[f"s{k}/density"] = np.asarray(st.density, float)
+        out[f"s{k}/denrot"] = np.asarray(st.denrot, float)
+    if params is not None:
+        for f in dataclasses.fields(params):
+            v = getattr(params, f.name)
+            out[f"params/{f.name}"] = np.array(v if not isinstance(v, tuple) else list(v))
+    np.savez_compressed(path, **out)
+
+
+def load_thldvec(path: str) -> tuple[list, dict]:
+    """Inverse of save_thldvec: (list of ThLenDenType, dict of the saved ParamSet fields)."""
+    with np.load(path) as d:
+        states = []
+        for k in range(int(d["nstates"])):
+            th = d[f"s{k}/theta"]
+            bodies = [ThetaLenType(th[i].copy(), float(d[f"s{k}/len"][i]), float(d[f"s{k}/xsm"][i]),
+                                   float(d[f"s{k}/ysm"][i]), float(d[f"s{k}/matau"][i])) for i in range(len(th))]
+            states.append(ThLenDenType(bodies, float(d[f"s{k}/tt"]), d[f"s{k}/density"].copy(),
+                                       d[f"s{k}/denrot"].copy()))
+        params = {k.split("/", 1)[1]: d[k][()] for k in d.files if k.startswith("params/")}
+    return states, params
+
+
 def new_thlenden(thlenvec) -> ThLenDenType:
     return ThLenDenType(list(thlenvec), 0.0)
 

@@ -78,3 +78,19 @@ def test_jld2_reader_matches_fixture():
         r, xc, yc = jld2.circles(f"/root/reference/simulations/input_geos/{name}.jld2")
         g = G.reference_input(name)
         assert np.array_equal(r, g.radii) and np.array_equal(xc, g.centers[:, 0])
+
+
+def test_state_file_round_trip(tmp_path):
+    from erosion_b200 import thetalen as TL
+    params = TL.ParamSet(npts=64, nouter=256)
+    st = TL.circs2thlenden(64, [0.3, 0.2], [-1.0, 0.5], [0.1, -0.2])
+    st.tt = 0.25
+    st.density = np.arange(5.0)
+    st.thlenvec[0].matau = 1.5
+    path = tmp_path / "run.npz"
+    TL.save_thldvec(str(path), [st, TL.circs2thlenden(64, [0.25], [0.0], [0.0])], params)
+    back, p = TL.load_thldvec(str(path))
+    assert len(back) == 2 and back[0].tt == 0.25
+    assert np.array_equal(back[0].thlenvec[1].theta, st.thlenvec[1].theta)
+    assert back[0].thlenvec[0].matau == 1.5 and np.array_equal(back[0].density, st.density)
+    assert int(p["npts"]) == 64 and tuple(p["wall"]) == G.REFERENCE_WALL
