@@ -713,6 +713,7 @@ k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
       __syncthreads();
     }
     const float d = 1.f / A[(size_t)k * m + k];
+    __syncthreads();   // every thread holds the pivot before row k is overwritten
     for (int j = tid; j < m; j += nt) {
       float v = (j == k) ? d : A[(size_t)k * m + j] * d;
       A[(size_t)k * m + j] = v;
