@@ -612,6 +612,10 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       EB_CK(cudaEventCreateWithFlags(&mb.ev_pre, cudaEventDisableTiming));
       EB_CK(cudaEventCreateWithFlags(&mb.ev_post, cudaEventDisableTiming));
       s.st = mb.side;
+      // the ensemble's far field runs in the ensemble's own launch shapes
+      // (tune_batch), so the members skip the per-geometry timing
+      s.force_shape[0] = 1;
+      s.force_shape[1] = 0;
       Problem pr;
       pr.P = P;
       if (npts[g] < 0 || nbods[g] < 0 || nouter[g] < 0) throw Error(EROSION_BAD_INPUT, "negative sizes");
