@@ -60,3 +60,30 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(_lib.ErosionError) as e:
         stokes.matvec(g, np.zeros(g.ntot))
     assert e.value.code == _lib.EROSION_NO_DEVICE
+
+
+@pytest.mark.parametrize("cname,pyname", [("erosion_params", "ErosionParams"), ("erosion_solve_stats", "SolveStats"),
+                                          ("erosion_batch_stats", "BatchStats"),
+                                          ("erosion_step_params", "StepParams"),
+                                          ("erosion_step_stats", "StepStats")])
+def test_struct_mirrors_match_the_header(tmp_path, cname, pyname):
+    """Every ctypes mirror has the size and field offsets the C compiler gives
+    the header's struct (the ABI a Julia or C caller sees)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    py = getattr(_lib, pyname)
+    fields = [f[0] for f in py._fields_]
+    src = tmp_path / "layout.c"
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "erosion_b200.h"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({cname}));']
+    lines += [f'  printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == ctypes.sizeof(py)
+    assert out[1:] == [getattr(py, f).offset for f in fields]
