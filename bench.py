@@ -7,13 +7,21 @@ two GMRES solves of the Stokes boundary integral equation to relative residual
 libstokes_b200.so on the GPU.  Synthetic seeded geometries of the named
 workloads (erosion_b200.geometry.workload); fixed pressure drop off.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2]
-                  [--impl ours|reference] [--precision 0|1] [--warm-start 0|1]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3]
+                  [--impl ours|reference] [--precision 0|1] [--warm-start 0|1|2]
 
 Prints one JSON line on rank 0.  `value` is device-timed (CUDA events on the
-library's stream) with the state resident in HBM; `e2e` goes through the
-host-array C-ABI entry point with the host<->device copies inside the timed
-region.  L2 is flushed (a 256 MiB write) before every timed step.
+library's stream) with the state resident in HBM; `e2e` repeats the same K
+steps from the same starting state through the host-array C-ABI entry point
+(erosion_rk2_step), the host<->device copies inside the timed region.  L2 is
+flushed (a 256 MiB write) before every timed step.  The body count is fixed
+over the timed window: the step dt is chosen so that no body erodes away, and
+should one be deleted all the same the state is restored to the window's
+starting state before the next step (counted in `config.restores`).  The
+far-field launch shapes are tuned during the warm-up and then frozen, so no
+tuning runs inside a timed region.  `plain_fp64` is one step of the
+reference's algorithm on the GPU (FP64 operator, no preconditioner, zero
+initial guess) from the same starting state.
 """
 from __future__ import annotations
 
@@ -34,45 +42,61 @@ sys.path.insert(0, ROOT)
 
 # dt: the workloads' stated steps (1e-3, 5e-4) delete every body within the
 # first step under the reference's erosion law in this channel (|tau| ~ 20-100,
-# dL/dt ~ -100..-600 against L ~ 0.2-0.7), so the step is scaled to 1e-5,
-# which keeps every body through the timed window.  The per-step work (two
-# solves, two shear stresses, the theta-L arithmetic) does not depend on dt.
+# dL/dt ~ -100..-1000 against L ~ 0.1-0.7), so the step is scaled down until
+# every body survives the warm-up, the timed window and the comparison legs.
+# The per-step work (two solves, two shear stresses, the theta-L arithmetic)
+# does not depend on dt.
 WORKLOADS = {
     "c1": dict(desc="10 circles x 128 nodes, 1024 wall nodes, channel [-1,1]x[-0.5,0.5], parabolic inflow",
                dt=1e-5, dt_config=1e-3),
     "c2": dict(desc="100 perturbed bodies x 256 nodes (25.6k body nodes), 2048 wall nodes, channel "
-                    "[-1,1]x[-0.5,0.5], parabolic inflow", dt=1e-5, dt_config=5e-4),
-    "c3": dict(desc="400 circles x 256 nodes (102k body nodes), 4096 wall nodes, channel [-1,1]x[-0.5,0.5]",
-               dt=1e-5, dt_config=5e-4),
-    "c5": dict(desc="200 circles x 256 nodes, 4096 wall nodes, channel [-1,1]x[-0.5,0.5]", dt=1e-5,
+                    "[-1,1]x[-0.5,0.5], parabolic inflow", dt=2e-6, dt_config=5e-4),
+    "c3": dict(desc="400 circles x 256 nodes (102k body nodes), 4096 wall nodes, channel [-1,1]x[-0.5,0.5], "
+                    "parabolic inflow", dt=1e-6, dt_config=5e-4),
+    "c5": dict(desc="200 circles x 256 nodes, 4096 wall nodes, channel [-1,1]x[-0.5,0.5]", dt=1e-6,
                dt_config=5e-4),
     # ensemble: a step is one ensemble solve (every geometry to 1e-8), not an erosion step
     "c4": dict(desc="ensemble of independent channel geometries, bodies U{20..200}, nodes per body "
                     "{128,256,512}, porosity U[0.5,0.8], 2048 wall nodes", dt=None, dt_config=None),
 }
 METRIC = "erosion steps/s at 1e-8 residual"
-ITER_FILE = os.path.join(ROOT, "profiles", "gmres_iterations.json")
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "far_field_traffic.json")
+
+# DRAM bytes per node and far-field launch (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch divided by the node count N) from the ncu
+# captures of the far-field kernels on the 100-body channel (N = 27,648):
+# both kernels read each source and target record once, so a launch moves
+# N x ~64 B at every size.
+TRAFFIC_BYTES_PER_NODE = {"k_far64": 1780224 / 27648, "k_far32": 1737472 / 27648,
+                          "k_far64_wall_sources": 1780224 / 27648}
+
+# Plain FP64 GMRES iterations per erosion step (unpreconditioned, zero initial
+# guess: the reference's algorithm) on the seeded workloads, as the plain_fp64
+# leg of this script measures them on the GPU.  Used only by the reference
+# arm's model for workloads whose CPU solve cannot finish in minutes; on c1
+# the reference arm runs the oracle's own GMRES instead.
+PLAIN_ITERATIONS_PER_STEP = {"c2": 3165, "c3": 12046, "c5": 6000}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", type=int, default=1, help="0 FP64, 1 mixed (FP32 far field + FP64 refinement)")
     ap.add_argument("--precond", type=int, default=1, help="0 none (reference), 1 block Gauss-Seidel")
-    ap.add_argument("--warm-start", type=int, default=0)
+    ap.add_argument("--warm-start", type=int, default=1,
+                    help="0 zero guess (the reference), 1 previous step's density, 2 also the learned guess")
+    ap.add_argument("--dt", type=float, default=None, help="override the workload's step")
     ap.add_argument("--compare-plain", type=int, default=1,
                     help="also time one step of the plain FP64 unpreconditioned form")
+    ap.add_argument("--e2e", type=int, default=1, help="time the host-array entry point over the same K steps")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ensemble", type=int, default=64, help="geometries of the c4 ensemble")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------
@@ -164,94 +188,145 @@ def max_over_ranks(x: float, dist, local: int = 0) -> float:
     return float(t.item())
 
 
-def cpu_rate(g, iters_per_step: float, budget_s: float, threads: int | None = None):
-    """Erosion steps/s of the oracle port on the host cores, from a bounded
-    sample: FP64 operator applications of the workload (mode: direct far field
-    + barycentric near field) and the shear stress on a sub-problem of the
-    first m bodies, scaled by M(M-1)/(m(m-1)).  Step = iterations x operator +
-    2 x stress (+ the O(M n^2) theta-L arithmetic, negligible)."""
-    from oracle import Oracle
+# ---------------------------------------------------------------------------
+# CPU side: the oracle port of the reference's path (the reference itself,
+# Julia + Fortran, cannot be built on this image).
+def cpu_operator_time(o, g, budget_s: float, max_apps: int = 20):
+    """Seconds per FP64 operator application of the oracle on workload g
+    (direct far field + barycentric near field, matvec_DLP_bary semantics with
+    the fmmbary near rules), averaged over as many applications as fit in
+    about budget_s (at least one)."""
+    den = np.random.default_rng(0).standard_normal(g.ntot)
+    t0 = time.perf_counter()
+    o.matvec(g, den, mode=1)
+    n = 1
+    while time.perf_counter() - t0 < budget_s and n < max_apps:
+        o.matvec(g, den, mode=1)
+        n += 1
+    return (time.perf_counter() - t0) / n, n
+
+
+def cpu_stress_model(o, g, sizes=(2, 4)):
+    """Seconds of the oracle's shear stress on workload g from two timed
+    sub-problems (the full wall with the first m bodies, m in sizes): the
+    reference's cost is a per-body wall part plus a per-ordered-pair part,
+    T(m) = a m + b m (m - 1), fitted to the two samples and evaluated at M."""
     from erosion_b200 import geometry as G
+    ts = []
+    for m in sizes:
+        m = min(m, g.M)
+        sub = G.Geometry(g.n, g.nout, g.xx[:m * g.n].copy(), g.yy[:m * g.n].copy(), g.wall, g.ibc, g.radii[:m],
+                         g.centers[:m])
+        d = np.random.default_rng(1).standard_normal(sub.ntot)
+        t0 = time.perf_counter()
+        o.shear_stress(sub, d)
+        ts.append((m, time.perf_counter() - t0))
+    (m1, t1), (m2, t2) = ts
+    if m1 == m2 or g.M <= m2:
+        return t2 * g.M / max(m2, 1), ts
+    A = np.array([[m1, m1 * (m1 - 1)], [m2, m2 * (m2 - 1)]], float)
+    a, b = np.linalg.solve(A, np.array([t1, t2]))
+    a, b = max(a, 0.0), max(b, 0.0)
+    return a * g.M + b * g.M * (g.M - 1), ts
+
+
+def cpu_rate(g, iters_per_step: float, budget_s: float, threads: int | None = None):
+    """Erosion steps/s of the oracle port on the host cores from a bounded
+    sample: FP64 operator applications of the workload and the two-point
+    shear-stress model.  Step = iterations x operator + 2 x stress (+ the
+    O(M n^2) theta-L arithmetic, negligible)."""
+    from oracle import Oracle
     o = Oracle()
     if threads:
         o.threads(threads)
     nthreads = o.threads()
-    den = np.random.default_rng(0).standard_normal(g.ntot)
-    t0 = time.perf_counter()
-    o.matvec(g, den, mode=1)
-    t_mv = time.perf_counter() - t0
-    nmv = 1
-    while time.perf_counter() - t0 < 0.4 * budget_s and nmv < 20:
-        o.matvec(g, den, mode=1)
-        nmv += 1
-    t_mv = (time.perf_counter() - t0) / nmv
-    m = min(g.M, 12)
-    sub = G.Geometry(g.n, g.nout, g.xx[:m * g.n].copy(), g.yy[:m * g.n].copy(), g.wall, g.ibc, g.radii[:m],
-                     g.centers[:m])
-    dsub = np.random.default_rng(1).standard_normal(sub.ntot)
-    t1 = time.perf_counter()
-    o.shear_stress(sub, dsub)
-    t_st_sub = time.perf_counter() - t1
-    scale = (g.M * (g.M - 1)) / max(m * (m - 1), 1)
-    t_stress = t_st_sub * scale
+    t_mv, nmv = cpu_operator_time(o, g, 0.5 * budget_s)
+    t_stress, ts = cpu_stress_model(o, g)
     t_step = iters_per_step * t_mv + 2 * t_stress
-    sample = (f"{nmv} FP64 operator applications of the full workload ({t_mv:.3f} s each) and one shear stress "
-              f"of its first {m} bodies ({t_st_sub:.2f} s, scaled x{scale:.1f}); step = {iters_per_step:.0f} "
-              f"GMRES iterations x operator + 2 stresses")
+    sample = (f"{nmv} FP64 operator applications of the full workload ({t_mv:.3f} s each) and the shear stress "
+              f"of the wall with the first {ts[0][0]} and {ts[1][0]} bodies ({ts[0][1]:.2f} s, {ts[1][1]:.2f} s; "
+              f"a m + b m(m-1) fit gives {t_stress:.1f} s at {g.M} bodies); step = {iters_per_step:.0f} GMRES "
+              f"iterations x operator + 2 stresses")
     return 1.0 / t_step, nthreads, sample, t_step
 
 
-def load_iterations(workload: str):
-    try:
-        with open(ITER_FILE) as f:
-            return json.load(f).get(workload)
-    except Exception:
-        return None
+def cpu_step_c1(o, g):
+    """One erosion step's solver work of the oracle at c1, run for real: two
+    GMRES solves to 1e-8 from zero (the oracle's SLATEC-semantics GMRES) and
+    two shear stresses.  Returns (seconds, GMRES iterations)."""
+    t0 = time.perf_counter()
+    it = 0
+    for _ in range(2):
+        den, nits, _, _ = o.solve(g, tol=1e-8)
+        it += nits
+        o.shear_stress(g, den)
+    return time.perf_counter() - t0, it
 
 
 def run_reference(args, world, rank):
     """The reference's own CPU path cannot be built here (Fortran + Julia);
-    this arm times the oracle port of it on all host cores."""
+    this arm times the oracle port of it on all host cores: a real step at c1,
+    a model from timed samples at the larger workloads."""
     if rank != 0:
         return
     if args.workload == "c4":
         print(json.dumps({"impl": "reference", "unavailable": "the reference arm is defined per geometry (c1-c3, "
-                                                              "c5); the ensemble has no recorded plain iteration "
-                                                              "counts to scale the CPU sample by"}))
+                                                              "c5); the ensemble has no plain iteration count to "
+                                                              "scale the CPU sample by"}))
         return
     from erosion_b200 import geometry as G
+    from oracle import Oracle
     g = G.workload(args.workload, seed=args.seed)
-    rec = load_iterations(args.workload)
-    if not rec:
-        print(json.dumps({"impl": "reference", "unavailable": f"no recorded GMRES iteration count for "
-                                                              f"{args.workload} in profiles/gmres_iterations.json"}))
-        return
-    iters = float(rec["iterations_per_step"])
-    per_step_budget = max(4.0, 60.0 / max(args.steps + args.warmup, 1))
+    o = Oracle()
+    nth = o.threads()
     vals = []
-    for i in range(args.warmup + args.steps):
-        v, nth, sample, t_step = cpu_rate(g, iters, per_step_budget)
-        if i >= args.warmup:
-            vals.append(v)
+    if args.workload == "c1":
+        for i in range(args.warmup + args.steps):
+            t, it = cpu_step_c1(o, g)
+            if i >= args.warmup:
+                vals.append(1.0 / t)
+        cb = {"kind": "port", "cores": nth, "timed": True,
+              "sample": f"two oracle GMRES solves to 1e-8 from zero ({it} iterations) and two shear stresses of the "
+                        f"full workload per step"}
+    else:
+        iters = float(PLAIN_ITERATIONS_PER_STEP[args.workload])
+        t_stress, ts = cpu_stress_model(o, g)
+        per_step = max(2.0, 150.0 / max(args.steps + args.warmup, 1))
+        for i in range(args.warmup + args.steps):
+            t_mv, nmv = cpu_operator_time(o, g, per_step, max_apps=4)
+            if i >= args.warmup:
+                vals.append(1.0 / (iters * t_mv + 2 * t_stress))
+        cb = {"kind": "port", "cores": nth, "timed": False,
+              "model": "step = plain GMRES iterations x timed operator application + 2 x shear stress (a m + "
+                       "b m(m-1) fit of two timed sub-problems)",
+              "iterations_per_step": iters,
+              "iterations_source": "plain FP64 GMRES iterations per step (unpreconditioned, zero guess) that this "
+                                   "script's plain_fp64 GPU leg measures on the same seeded workload",
+              "sample": f"{nmv} oracle FP64 operator applications of the full workload per step ({t_mv:.2f} s each); "
+                        f"shear stress of the wall with {ts[0][0]} and {ts[1][0]} bodies ({ts[0][1]:.2f} s, "
+                        f"{ts[1][1]:.2f} s)"}
     v = float(np.mean(vals))
+    cb["value"] = v
+    cb["unit"] = "steps/s"
     out = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}",
+                      "bodies": g.M, "nodes_per_body": g.n, "wall_nodes": g.nout, "tol": 1e-8,
                       "parallelism": "host threads (OpenMP)"},
-           "impl": "reference",
-           "cpu_baseline": {"value": v, "unit": "steps/s", "cores": nth, "kind": "port", "sample": sample},
+           "impl": "reference", "cpu_baseline": cb,
            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------------------
 def run_ensemble(args, world, rank, local, dist):
     """The batching workload: one step = one solve of every geometry of an
     ensemble to 1e-8 (mixed precision, block preconditioner) through
     erosion_solve_batch, host arrays in and out.  Reported as GMRES solves/s
     beside the same geometries solved one erosion_solve call after another."""
     import torch
-    from erosion_b200 import _lib, geometry as G, stokes
+    from erosion_b200 import geometry as G, stokes
     E = G.ensemble(args.ensemble, seed=args.seed + rank)
     kw = dict(precision=args.precision, precond=args.precond)
     for _ in range(args.warmup):
@@ -297,66 +372,114 @@ def run_ensemble(args, world, rank, local, dist):
         print(json.dumps(line))
 
 
-def main():
-    args = parse()
-    world, rank, local, dist = dist_setup(args)
-    if args.impl == "reference":
-        run_reference(args, world, rank)
-        if dist:
-            dist.destroy_process_group()
-        return
-    import torch
-    from erosion_b200 import _lib, build, geometry as G
-    build.build()
-    L = _lib.load()
-    torch.cuda.set_device(local)
-    if args.workload == "c4":
-        run_ensemble(args, world, rank, local, dist)
-        if dist:
-            dist.destroy_process_group()
-        return
-    dev = torch.device("cuda", local)
+# ---------------------------------------------------------------------------
+class Stepper:
+    """The theta-L state of one workload on the device, stepped through
+    erosion_rk2_step_device, with snapshot/restore of the starting state."""
 
-    wl = WORKLOADS[args.workload]
-    g = G.workload(args.workload, seed=args.seed + rank)
-    th, ln, xs, ys = G.to_thetalen(g)
-    M0, n = g.M, g.n
-    p = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=args.precision, precond=args.precond)
-    p_plain = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=0, precond=0)
-    sp = _lib.StepParams()
-    L.erosion_default_step_params(ctypes.byref(sp), n)
-    sp.dt = wl["dt"]
-    sp.fixpdrop = 0
-    sp.warm_start = args.warm_start
+    def __init__(self, L, g, dev, dt, warm_start):
+        import torch
+        from erosion_b200 import _lib, geometry as G
+        self.L, self.g, self.torch, self._lib = L, g, torch, _lib
+        th, ln, xs, ys = G.to_thetalen(g)
+        self.n = g.n
+        self.d = [torch.tensor(a, dtype=torch.float64, device=dev) for a in (th, ln, xs, ys)]
+        self.nb = np.array([g.M], np.int64)
+        self.tt = np.zeros(1)
+        self.deleted = np.zeros(g.M, np.int64)
+        self.sp = _lib.StepParams()
+        L.erosion_default_step_params(ctypes.byref(self.sp), g.n)
+        self.sp.dt = dt
+        self.sp.fixpdrop = 0
+        self.sp.warm_start = warm_start
+        self.snap = None
 
-    d_th = torch.tensor(th, dtype=torch.float64, device=dev)
-    d_ln = torch.tensor(ln, dtype=torch.float64, device=dev)
-    d_xs = torch.tensor(xs, dtype=torch.float64, device=dev)
-    d_ys = torch.tensor(ys, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.ExternalStream(L.erosion_stream(), device=dev)
-    nb = np.array([M0], np.int64)
-    tt = np.zeros(1)
-    deleted = np.zeros(M0, np.int64)
-    PI64, PD = _lib.PI64, _lib.PD
+    @property
+    def M(self) -> int:
+        return int(self.nb[0])
 
-    def step(params=None):
-        params = params or p
-        rc = L.erosion_rk2_step_device(ctypes.byref(params), ctypes.byref(sp), n, nb.ctypes.data_as(PI64), g.nout,
-                                       d_th.data_ptr(), d_ln.data_ptr(), d_xs.data_ptr(), d_ys.data_ptr(),
-                                       tt.ctypes.data_as(PD), deleted.ctypes.data_as(PI64))
+    def step(self, params, sp=None):
+        _lib = self._lib
+        sp = sp or self.sp
+        th, ln, xs, ys = self.d
+        rc = self.L.erosion_rk2_step_device(ctypes.byref(params), ctypes.byref(sp), self.n,
+                                            self.nb.ctypes.data_as(_lib.PI64), self.g.nout, th.data_ptr(),
+                                            ln.data_ptr(), xs.data_ptr(), ys.data_ptr(),
+                                            self.tt.ctypes.data_as(_lib.PD), self.deleted.ctypes.data_as(_lib.PI64))
         _lib.check(rc, (_lib.EROSION_OK, _lib.EROSION_MAXITER))
         st = _lib.StepStats()
-        L.erosion_get_step_stats(ctypes.byref(st))
+        self.L.erosion_get_step_stats(ctypes.byref(st))
         return st.as_dict()
+
+    def snapshot(self):
+        self.snap = ([a.clone() for a in self.d], int(self.nb[0]), float(self.tt[0]))
+
+    def restore(self):
+        arrs, M, t = self.snap
+        for a, s in zip(self.d, arrs):
+            a.copy_(s)
+        self.nb[0] = M
+        self.tt[0] = t
+
+    def host_state(self):
+        """The snapshot as host arrays (the e2e leg's input)."""
+        arrs, M, _ = self.snap
+        n = self.n
+        return (arrs[0][: M * n].cpu().numpy().copy(), arrs[1][:M].cpu().numpy().copy(),
+                arrs[2][:M].cpu().numpy().copy(), arrs[3][:M].cpu().numpy().copy())
+
+
+def kernel_roofline(s0, s1, N, peak64, peak32, ms_timed):
+    """Per far-field kernel: launches, time, pairs per launch, achieved
+    TFLOP/s (20 flops per pair), fraction of the measured FMA peak of its pipe
+    and the DRAM bytes per launch (ncu figure per node x N)."""
+    kernels = {}
+    spec = (("k_far64", "ms_far", "far_launches", "far64_pairs", peak64),
+            ("k_far64_wall_sources", "ms_farw", "farw_launches", "farw_pairs", peak64),
+            ("k_far32", "ms_far32", "far32_launches", "far32_pairs", peak32))
+    for name, kms, kn, kp, peak in spec:
+        ms = s1[kms] - s0[kms]
+        nl = s1[kn] - s0[kn]
+        if nl <= 0:
+            continue
+        pairs = s1[kp]
+        a = 20.0 * pairs / (ms / nl * 1e-3) / 1e12
+        kernels[name] = {"launches": nl, "ms_total": ms, "ms_avg": ms / nl, "pairs_per_launch": pairs,
+                         "achieved_tflops": a, "peak_tflops": peak, "frac": a / peak,
+                         "share_of_timed": ms / ms_timed,
+                         "traffic_bytes_per_launch": TRAFFIC_BYTES_PER_NODE[name] * N,
+                         "algorithmic_bytes_per_launch": 64 * N}
+    return kernels
+
+
+def run_steps(args, world, rank, local, dist):
+    import torch
+    from erosion_b200 import _lib, geometry as G
+    L = _lib.load()
+    dev = torch.device("cuda", local)
+    wl = WORKLOADS[args.workload]
+    dt = args.dt if args.dt is not None else wl["dt"]
+    g = G.workload(args.workload, seed=args.seed + rank)
+    p = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=args.precision, precond=args.precond)
+    p_plain = _lib.default_params(wall=tuple(g.wall), ibc=g.ibc, precision=0, precond=0)
+    S = Stepper(L, g, dev, dt, args.warm_start)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(L.erosion_stream(), device=dev)
 
     def solve_stats():
         s = _lib.SolveStats()
         L.erosion_get_solve_stats(ctypes.byref(s))
         return s.as_dict()
 
+    M_start0 = S.M
     for _ in range(args.warmup):
-        step()
+        S.step(p)
+    # freeze the launch shapes the warm-up tuned
+    shapes = _lib.far_shapes()
+    L.erosion_set_far_shape(0, shapes["fp64"]["index"])
+    L.erosion_set_far_shape(1, shapes["fp32"]["index"])
+    S.snapshot()
+    M0 = S.M
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -365,154 +488,176 @@ def main():
     launches0 = L.erosion_launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    iters = []
-    per_step = []
+    per_step, restores, deleted = [], 0, 0
     with Clocks(local) as clk:
         with torch.cuda.stream(stream):
             ev0.record(stream)
             for _ in range(args.steps):
                 flush.zero_()
-                st = step()
-                iters.append(sum(st["gmres_iterations"]))
+                st = S.step(p)
                 per_step.append(st)
+                if S.M != M0:
+                    deleted += M0 - S.M
+                    S.restore()
+                    restores += 1
             ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     launches = L.erosion_launch_count() - launches0
     s1 = solve_stats()
+    M_end = S.M
     ms = max_over_ranks(ms, dist, local)
     value = world * args.steps / (ms * 1e-3)
-
-    # roofline of the dominant far-field kernel: FP64 (k_far64) or FP32
-    # (k_far32), against the measured FMA peak of the pipe it runs on
-    N = g.nout + n * int(nb[0])
-    far64_ms = s1["ms_far"] - s0["ms_far"]
-    far64_n = s1["far_launches"] - s0["far_launches"]
-    far32_ms = s1["ms_far32"] - s0["ms_far32"]
-    far32_n = s1["far32_launches"] - s0["far32_launches"]
+    N = g.nout + g.n * M0
     peak64 = L.erosion_peak_tflops(0)
     peak32_scalar = L.erosion_peak_tflops(1)
     peak32_packed = L.erosion_peak_tflops(2)
-    peak32 = max(peak32_scalar, peak32_packed)   # the higher of scalar and two-lane FMA
-    kernels = {}
-    if far64_n:
-        a = 20.0 * s1["far64_pairs"] / (far64_ms / far64_n * 1e-3) / 1e12
-        kernels["k_far64"] = {"launches": far64_n, "ms_total": far64_ms, "ms_avg": far64_ms / far64_n,
-                              "pairs_per_launch": s1["far64_pairs"], "achieved_tflops": a, "peak_tflops": peak64,
-                              "frac": a / peak64, "share_of_timed": far64_ms / ms}
-    farw_ms = s1["ms_farw"] - s0["ms_farw"]
-    farw_n = s1["farw_launches"] - s0["farw_launches"]
-    if farw_n:
-        a = 20.0 * s1["farw_pairs"] / (farw_ms / farw_n * 1e-3) / 1e12
-        kernels["k_far64_wall_sources"] = {"launches": farw_n, "ms_total": farw_ms, "ms_avg": farw_ms / farw_n,
-                                           "pairs_per_launch": s1["farw_pairs"], "achieved_tflops": a,
-                                           "peak_tflops": peak64, "frac": a / peak64, "share_of_timed": farw_ms / ms}
-    if far32_n:
-        pairs32 = s1["far32_pairs"]
-        a = 20.0 * pairs32 / (far32_ms / far32_n * 1e-3) / 1e12
-        kernels["k_far32"] = {"launches": far32_n, "ms_total": far32_ms, "ms_avg": far32_ms / far32_n,
-                              "pairs_per_launch": pairs32, "achieved_tflops": a, "peak_tflops": peak32,
-                              "frac": a / peak32, "share_of_timed": far32_ms / ms}
+    peak32 = max(peak32_scalar, peak32_packed)
+    kernels = kernel_roofline(s0, s1, N, peak64, peak32, ms)
     dom = max(kernels, key=lambda k: kernels[k]["ms_total"]) if kernels else None
-    traffic = None
-    try:
-        with open(TRAFFIC_FILE) as f:
-            traffic = json.load(f).get(f"{args.workload}:{dom}") or json.load(open(TRAFFIC_FILE)).get(args.workload)
-    except Exception:
-        pass
-    roofline = {"bound": "fp32" if dom == "k_far32" else "fp64", "achieved": kernels[dom]["achieved_tflops"] if dom else None,
+    roofline = {"bound": ("fp32" if dom == "k_far32" else "fp64") if dom else None,
+                "achieved": kernels[dom]["achieved_tflops"] if dom else None,
                 "peak": kernels[dom]["peak_tflops"] if dom else None, "unit": "TFLOP/s",
-                "frac": kernels[dom]["frac"] if dom else None, "traffic": traffic, "kernel": dom,
+                "frac": kernels[dom]["frac"] if dom else None,
+                "traffic": kernels[dom]["traffic_bytes_per_launch"] if dom else None, "kernel": dom,
                 "algorithmic": "20 flops per source-target pair; pairs per launch: k_far64 = node pairs of distinct "
                                "curves less the barycentric near pairs (self-curve pairs run in k_self64); in the "
                                "mixed operator k_far32 takes the body-source pairs and k_far64_wall_sources the "
                                "wall-source pairs",
-                "peak_source": "measured FMA loop on this GPU (erosion_peak_tflops), vector pipe; FP32 = max of "
+                "peak_source": "of measured: FMA loop on this GPU (erosion_peak_tflops), vector pipe; FP32 = max of "
                                "scalar and packed two-lane FMA",
-                "peaks_measured_tflops": {"fp64": peak64, "fp32_scalar": peak32_scalar, "fp32_packed": peak32_packed},
-                "launch_shapes": _lib.far_shapes(),
-                "kernels": kernels}
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch of the ncu capture on "
+                                  "the 100-body channel, per node, times N",
+                "peaks_measured_tflops": {"fp64": peak64, "fp32_scalar": peak32_scalar,
+                                          "fp32_packed": peak32_packed},
+                "launch_shapes": shapes, "kernels": kernels}
+    mv = sum(sum(st["matvecs"]) for st in per_step)
+    mv32 = sum(sum(st["matvecs_fp32"]) for st in per_step)
 
-    # end to end through the host-array entry point (state in host memory)
+    # end to end: the same K steps from the same starting state through the
+    # host-array entry point
     e2e = None
-    if args.e2e_steps > 0:
-        hth = d_th[: int(nb[0]) * n].cpu().numpy().copy()
-        hln = d_ln[: int(nb[0])].cpu().numpy().copy()
-        hxs = d_xs[: int(nb[0])].cpu().numpy().copy()
-        hys = d_ys[: int(nb[0])].cpu().numpy().copy()
-        Mh = np.array([int(nb[0])], np.int64)
+    if args.e2e:
+        hth, hln, hxs, hys = S.host_state()
+        Mh = np.array([M0], np.int64)
+        tt = np.zeros(1)
+        dl = np.zeros(M0, np.int64)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         h2d = d2h = 0
+        t0 = time.perf_counter()
         with torch.cuda.stream(stream):
             e0.record(stream)
-            for _ in range(args.e2e_steps):
+            for _ in range(args.steps):
                 flush.zero_()
-                Mcur = int(Mh[0])
-                h2d += (Mcur * n + 3 * Mcur) * 8
-                rc = L.erosion_rk2_step(ctypes.byref(p), ctypes.byref(sp), n, Mh.ctypes.data_as(PI64), g.nout,
-                                        _lib.ptr(hth), _lib.ptr(hln), _lib.ptr(hxs), _lib.ptr(hys),
-                                        tt.ctypes.data_as(PD), deleted.ctypes.data_as(PI64))
+                Mc = int(Mh[0])
+                h2d += (Mc * g.n + 3 * Mc) * 8
+                rc = L.erosion_rk2_step(ctypes.byref(p), ctypes.byref(S.sp), g.n, Mh.ctypes.data_as(_lib.PI64),
+                                        g.nout, _lib.ptr(hth), _lib.ptr(hln), _lib.ptr(hxs), _lib.ptr(hys),
+                                        tt.ctypes.data_as(_lib.PD), dl.ctypes.data_as(_lib.PI64))
                 _lib.check(rc, (_lib.EROSION_OK, _lib.EROSION_MAXITER))
-                d2h += (int(Mh[0]) * n + 3 * int(Mh[0])) * 8
+                d2h += (int(Mh[0]) * g.n + 3 * int(Mh[0])) * 8
             e1.record(stream)
         torch.cuda.synchronize()
+        wall_e2e = time.perf_counter() - t0
         ems = max_over_ranks(e0.elapsed_time(e1), dist, local)
-        e2e = {"value": world * args.e2e_steps / (ems * 1e-3), "unit": "steps/s",
-               "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
-               "entry_point": "erosion_rk2_step (host arrays)"}
+        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": "steps/s", "steps": args.steps,
+               "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+               "entry_point": "erosion_rk2_step (host arrays), same starting state and step count as value",
+               "host_wall_s": wall_e2e, "bodies_end": int(Mh[0])}
 
-    mean_iters = float(np.mean(iters)) if iters else 0.0
     plain = None
     if args.compare_plain:
+        S.restore()
+        sp_plain = _lib.StepParams()
+        ctypes.memmove(ctypes.byref(sp_plain), ctypes.byref(S.sp), ctypes.sizeof(sp_plain))
+        sp_plain.warm_start = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         sp0 = solve_stats()
         with torch.cuda.stream(stream):
             flush.zero_()
             e0.record(stream)
-            stp = step(p_plain)
+            stp = S.step(p_plain, sp_plain)
             e1.record(stream)
         torch.cuda.synchronize()
-        pms = e0.elapsed_time(e1)
+        pms = max_over_ranks(e0.elapsed_time(e1), dist, local)
         sp1 = solve_stats()
-        plain = {"value": 1.0 / (pms * 1e-3) * world, "unit": "steps/s", "steps": 1,
+        pv = world / (pms * 1e-3)
+        plain = {"value": pv, "unit": "steps/s", "steps": 1,
                  "gmres_iterations_per_step": sum(stp["gmres_iterations"]),
                  "step_breakdown_ms": {k: stp[k] for k in ("ms_solve", "ms_stress", "ms_thetalen", "ms_total")},
                  "far64_ms": sp1["ms_far"] - sp0["ms_far"],
-                 "form": "FP64 operator, no preconditioner, zero initial guess (the reference's algorithm)",
-                 "speedup_of_value": value / (1.0 / (pms * 1e-3) * world)}
+                 "form": "FP64 operator, no preconditioner, zero initial guess (the reference's algorithm), from "
+                         "the timed window's starting state",
+                 "speedup_of_value": value / pv,
+                 "speedup_of_e2e": (e2e["value"] / pv) if e2e else None}
+    L.erosion_set_far_shape(0, -1)
+    L.erosion_set_far_shape(1, -1)
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            it_ref = plain["gmres_iterations_per_step"] if plain else (load_iterations(args.workload) or {}).get(
-                "iterations_per_step", mean_iters)
+            it_ref = plain["gmres_iterations_per_step"] if plain else PLAIN_ITERATIONS_PER_STEP.get(args.workload, 0)
             v, nth, sample, t_step = cpu_rate(g, it_ref, args.cpu_seconds)
-            cpu = {"value": v, "unit": "steps/s", "cores": nth, "kind": "port", "sample": sample}
+            cpu = {"value": v, "unit": "steps/s", "cores": nth, "kind": "port", "sample": sample, "timed": False,
+                   "iterations_source": "this run's plain_fp64 leg" if plain else "PLAIN_ITERATIONS_PER_STEP"}
         pairs_per_s = (s1["matvecs"] - s0["matvecs"]) * N * (N - 1) / (ms * 1e-3) * world
+        iters = [sum(st["gmres_iterations"]) for st in per_step]
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f64+f32",
                "data": "synthetic",
-               "config": {"workload": f"{args.workload}: {wl['desc']}", "bodies": M0, "nodes_per_body": n,
-                          "wall_nodes": g.nout, "unknowns": g.ntot, "dt": wl["dt"],
-                          "dt_note": f"configured dt {wl['dt_config']} deletes every body in step 1 at this "
-                                     f"shear-stress scale; scaled to keep the bodies", "fixpdrop": 0, "tol": 1e-8,
+               "config": {"workload": f"{args.workload}: {wl['desc']}", "bodies": M_start0,
+                          "bodies_start": M0, "bodies_end": M_end, "bodies_deleted_in_window": deleted,
+                          "restores": restores, "nodes_per_body": g.n, "wall_nodes": g.nout,
+                          "unknowns": 2 * N + 3 * M0, "dt": dt,
+                          "dt_note": f"configured dt {wl['dt_config']} deletes every body within the first step at "
+                                     f"this shear-stress scale; scaled so that every body survives the run",
+                          "fixpdrop": 0, "tol": 1e-8,
                           "precision": "fp64" if args.precision == 0 else "mixed", "warm_start": args.warm_start,
                           "precond": "block Gauss-Seidel" if args.precond else "none",
+                          "launch_shapes": "tuned in the warm-up, frozen for the timed regions",
                           "parallelism": "replicas" if world > 1 else "single GPU",
                           "l2": "flushed (256 MiB write) before every step"},
-               "gmres_iterations_per_step": mean_iters,
+               "gmres_iterations_per_step": float(np.mean(iters)) if iters else 0.0,
+               "gmres_iterations_per_solve": [i for st in per_step for i in st["gmres_iterations"]],
+               "far_field_launches": {"total": mv, "fp32": mv32, "fp32_share": mv32 / mv if mv else None},
                "pair_interactions_per_s": pairs_per_s,
                "gmres_solves_per_s": 2 * value,
                "step_breakdown_ms": {k: float(np.mean([s[k] for s in per_step])) for k in
-                                     ("ms_solve", "ms_stress", "ms_thetalen", "ms_total")},
+                                     ("ms_solve", "ms_stress", "ms_thetalen", "ms_total", "ms_setup",
+                                      "ms_precond_setup")},
+               "preconditioner": {"active_every_solve": all(a for st in per_step for a in st["precond_active"]),
+                                  "singular_blocks_max": max(b for st in per_step
+                                                             for b in st["precond_singular_blocks"]),
+                                  "setup_ms_per_step": float(np.mean([s["ms_precond_setup"] for s in per_step]))},
+               "guess_used": [u for st in per_step for u in st["guess_used"]],
                "plain_fp64": plain,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
-    if dist:
-        dist.destroy_process_group()
+
+
+def main(argv=None):
+    args = parse(argv)
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+            return
+        import torch
+        from erosion_b200 import _lib, build
+        build.build()
+        _lib.load()
+        torch.cuda.set_device(local)
+        if args.workload == "c4":
+            run_ensemble(args, world, rank, local, dist)
+        else:
+            run_steps(args, world, rank, local, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -86,6 +86,10 @@ class SolveStats(ctypes.Structure):
         ("ms_farw", c_double),
         ("farw_launches", c_int64),
         ("farw_pairs", c_int64),
+        ("precond_active", c_int64),
+        ("precond_singular_blocks", c_int64),
+        ("ms_setup", c_double),
+        ("ms_precond_setup", c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -124,13 +128,19 @@ class StepStats(ctypes.Structure):
     _fields_ = [("gmres_iterations", c_int64 * 2), ("bodies_deleted", c_int64),
                 ("ms_solve", c_double), ("ms_stress", c_double), ("ms_thetalen", c_double),
                 ("ms_total", c_double), ("max_residual", c_double), ("matau", c_double * 2),
-                ("guess_used", c_int64 * 2), ("guess_residual", c_double * 2)]
+                ("guess_used", c_int64 * 2), ("guess_residual", c_double * 2),
+                ("ms_setup", c_double), ("ms_precond_setup", c_double), ("precond_active", c_int64 * 2),
+                ("precond_singular_blocks", c_int64 * 2), ("matvecs", c_int64 * 2), ("matvecs_fp32", c_int64 * 2)]
 
     def as_dict(self) -> dict:
         return {"gmres_iterations": list(self.gmres_iterations), "bodies_deleted": self.bodies_deleted,
                 "ms_solve": self.ms_solve, "ms_stress": self.ms_stress, "ms_thetalen": self.ms_thetalen,
                 "ms_total": self.ms_total, "max_residual": self.max_residual, "matau": list(self.matau),
-                "guess_used": list(self.guess_used), "guess_residual": list(self.guess_residual)}
+                "guess_used": list(self.guess_used), "guess_residual": list(self.guess_residual),
+                "ms_setup": self.ms_setup, "ms_precond_setup": self.ms_precond_setup,
+                "precond_active": list(self.precond_active),
+                "precond_singular_blocks": list(self.precond_singular_blocks),
+                "matvecs": list(self.matvecs), "matvecs_fp32": list(self.matvecs_fp32)}
 
 
 # Every entry point declared in include/erosion_b200.h, with its signature.
@@ -168,6 +178,8 @@ SIGNATURES = {
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         PD, PI64]),
     "erosion_getxy": (c_int, [c_int64, c_int64, PD, PD, PD, PD, PD, PD]),
+    "erosion_drag": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD, PD, c_int32,
+                             c_double, PD, PD, PD, PD, PD]),
     "erosion_stream": (ctypes.c_void_p, []),
     "erosion_lw_features": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32]),
     "erosion_lw_encode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PF32]),

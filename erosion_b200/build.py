@@ -46,16 +46,37 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
+COMPILE_FLAGS = [*ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object file (in parallel: the kernels of
+    each file have internal linkage, so no relocatable device code is needed)
+    and links the shared library."""
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc_path(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr",
-           "-Xcompiler", "-fPIC", "-shared", "-I", INCLUDE, "-I", CSRC, "-o", OUT + ".tmp", *sources()]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    nvcc = nvcc_path()
+    jobs = []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        jobs.append((obj, [nvcc, *COMPILE_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", "-o", obj, src]))
     if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        for _, cmd in jobs:
+            print(" ".join(cmd))
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[1], capture_output=True, text=True), jobs))
+    for (obj, cmd), r in zip(jobs, results):
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    link = [nvcc, *ARCH_FLAGS, "-shared", "-o", OUT + ".tmp", *[o for o, _ in jobs]]
+    if verbose:
+        print(" ".join(link))
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -726,14 +726,12 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
     }
     B.stats.geometries = nbatch;
     EB_CK(cudaStreamSynchronize(st));
-    lib.status = worst;
-    lib.err = worst == EROSION_OK ? "" : "a geometry of the ensemble did not converge";
+    set_status(worst, worst == EROSION_OK ? "" : "a geometry of the ensemble did not converge");
     return worst;
   } catch (const Error& e) {
     if (lib.st) cudaStreamSynchronize(lib.st);
     destroy_graph(batch());
-    lib.status = e.code;
-    lib.err = e.what();
+    set_status(e.code, e.what());
     return e.code;
   }
 }

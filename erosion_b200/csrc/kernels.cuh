@@ -210,13 +210,18 @@ __device__ __forceinline__ double rcp_or_zero(double r2) { return r2 > 0.0 ? __d
 
 // 1/r2 for r2 > 0 by Newton-Raphson: the FP32 hardware reciprocal estimate
 // (relative error ~2^-23), refined twice by y <- y + y (1 - r2 y) in FP64
-// (quadratic convergence: ~2^-46, then below FP64 rounding).  r2 spans
-// ~1e-10..1e2 here, well inside FP32's normal range.  Not correctly rounded
-// (a last-bit difference from the division), which the operator's 1e-11
-// parity bound absorbs.
+// (quadratic convergence: ~2^-46, then below FP64 rounding).  Not correctly
+// rounded (a last-bit difference from the division), which the operator's
+// 1e-11 parity bound absorbs.
+// Valid range: FP32's normal range, 1.2e-38 <= r2 <= 3.4e38 (node distances
+// here give r2 ~ 1e-10..1e2).  The seed's argument is clamped to that range,
+// so r2 outside it returns a finite value (a wrong one: the seed is then too
+// far from 1/r2 for two Newton steps), never the NaN/inf that an
+// underflowing or overflowing FP32 conversion would give.
 __device__ __forceinline__ double rcp_newton(double r2) {
   float yf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(r2)));
+  const float r2f = fminf(fmaxf(__double2float_rn(r2), 1.17549435e-38f), 3.40282347e38f);
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(r2f));
   double y = (double)yf;
   double e = fma(-r2, y, 1.0);
   y = fma(y, e, y);
@@ -333,6 +338,25 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t) {
   lo += e;
 }
 
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// two_sum_add on two lanes at once (two targets), each lane exactly the
+// scalar form.
+__device__ __forceinline__ void two_sum_add2(float2& hi, float2& lo, float2 t) {
+  const float2 s = __fadd2_rn(hi, t);
+  const float2 bp = __fadd2_rn(s, neg2(hi));
+  const float2 e = __fadd2_rn(__fadd2_rn(hi, neg2(__fadd2_rn(s, neg2(bp)))), __fadd2_rn(t, neg2(bp)));
+  hi = s;
+  lo = __fadd2_rn(lo, e);
+}
+
+// Sources per FP32 partial sum of k_far32: the running FP32 sum of a target is
+// folded into its two-sum accumulator after every F32_CHUNK sources, so the
+// rounding error of the plain FP32 accumulation grows with the chunk length
+// instead of the tile length (measured on solution densities: the operator's
+// FP32 error is ~2.5x smaller with chunks of 16 than with whole 256-node tiles).
+constexpr int F32_CHUNK = 16;
+
 // One CTA's share of the FP32 far field (targets of block bx, tiles of split
 // 'split'); shared by k_far32 and the ensemble kernel k_far32_batch.
 template <bool MASK, int NT, int TPT, int U>
@@ -343,17 +367,19 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
                                           const unsigned* __restrict__ mask, int mw, double2* __restrict__ partial,
                                           int bx, int split, float4* s_pos, float4* s_nrm, float4* s_den) {
   static_assert(TPT % 2 == 0, "targets are processed in lane pairs");
+  static_assert(F32_CHUNK % U == 0, "the source-loop unroll divides the chunk");
   constexpr int TP = TPT / 2;
   const int i0 = bx * (NT * TPT) + threadIdx.x;
   int it[TPT], cv[TPT];
-  float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
+  float2 HX[TP], LX[TP], HY[TP], LY[TP];   // two-sum accumulators, lanes = targets 2p, 2p+1
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
     int i = i0 + q * NT;
     it[q] = i < N ? i : N - 1;
     cv[q] = it[q] < nout ? 0 : 1 + (it[q] - nout) / n;
-    hx[q] = lx[q] = hy[q] = ly[q] = 0.f;
   }
+#pragma unroll
+  for (int p = 0; p < TP; ++p) HX[p] = LX[p] = HY[p] = LY[p] = make_float2(0.f, 0.f);
   const int tb = split_ptr[split], te = split_ptr[split + 1];
   for (int ti = tb; ti < te; ++ti) {
     const int4 T = tiles[ti];
@@ -365,9 +391,18 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
       s_nrm[k] = make_float4(a.z, a.z, a.w, a.w);
       s_den[k] = make_float4(w.x, w.x, w.y, w.y);
     }
+    // pad the last chunk with zero-strength sources far from every target
+    // (exactly zero terms)
+    const int tlen = (T.y + F32_CHUNK - 1) / F32_CHUNK * F32_CHUNK;
+    for (int k = T.y + threadIdx.x; k < tlen; k += NT) {
+      s_pos[k] = make_float4(-1e4f, -1e4f, -1e4f, -1e4f);
+      s_nrm[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      s_den[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     __syncthreads();
     const double2 cs = tile_c[ti];
-    float2 PX[TP], PY[TP], TX[TP], TY[TP];
+    float2 PX[TP], PY[TP];
+    bool U0[TP], U1[TP];   // false: the pair is masked out of this tile (own curve or near)
 #pragma unroll
     for (int p = 0; p < TP; ++p) {
       const int q0 = it[2 * p], q1 = it[2 * p + 1];
@@ -375,41 +410,51 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
       const float2 o0 = tgt[q0], o1 = tgt[q1];
       PX[p] = make_float2((float)(a0.x - cs.x) + o0.x, (float)(a1.x - cs.x) + o1.x);
       PY[p] = make_float2((float)(a0.y - cs.y) + o0.y, (float)(a1.y - cs.y) + o1.y);
-      TX[p] = make_float2(0.f, 0.f);
-      TY[p] = make_float2(0.f, 0.f);
-    }
-#pragma unroll U
-    for (int j = 0; j < T.y; ++j) {
-      const float4 A = s_pos[j], B = s_nrm[j], C = s_den[j];
-      const float2 msx = make_float2(A.x, A.y), msy = make_float2(A.z, A.w);
-      const float2 nx = make_float2(B.x, B.y), ny = make_float2(B.z, B.w);
-      const float2 wx = make_float2(C.x, C.y), wy = make_float2(C.z, C.w);
-#pragma unroll
-      for (int p = 0; p < TP; ++p) {
-        const float2 rx = __fadd2_rn(PX[p], msx);
-        const float2 ry = __fadd2_rn(PY[p], msy);
-        const float2 rho2 = __ffma2_rn(rx, rx, __fmul2_rn(ry, ry));
-        const float2 rdn = __ffma2_rn(rx, nx, __fmul2_rn(ry, ny));
-        const float2 rds = __ffma2_rn(rx, wx, __fmul2_rn(ry, wy));
-        const float2 inv = make_float2(rcp_approx(rho2.x), rcp_approx(rho2.y));
-        const float2 c = __fmul2_rn(__fmul2_rn(rdn, rds), __fmul2_rn(inv, inv));
-        TX[p] = __ffma2_rn(c, rx, TX[p]);
-        TY[p] = __ffma2_rn(c, ry, TY[p]);
+      bool u0 = T.z != cv[2 * p], u1 = T.z != cv[2 * p + 1];
+      if (MASK) {
+        u0 = u0 && !((__ldg(mask + (size_t)q0 * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
+        u1 = u1 && !((__ldg(mask + (size_t)q1 * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
       }
+      U0[p] = u0;
+      U1[p] = u1;
     }
+    for (int j0 = 0; j0 < tlen; j0 += F32_CHUNK) {
+      float2 TX[TP], TY[TP];
 #pragma unroll
-    for (int q = 0; q < TPT; ++q) {
-      bool use = T.z != cv[q];
-      if (MASK) use = use && !((__ldg(mask + (size_t)it[q] * mw + (T.z >> 5)) >> (T.z & 31)) & 1u);
-      const float tx = (q & 1) ? TX[q >> 1].y : TX[q >> 1].x;
-      const float ty = (q & 1) ? TY[q >> 1].y : TY[q >> 1].x;
-      if (use) { two_sum_add(hx[q], lx[q], tx); two_sum_add(hy[q], ly[q], ty); }
+      for (int p = 0; p < TP; ++p) TX[p] = TY[p] = make_float2(0.f, 0.f);
+#pragma unroll U
+      for (int j = j0; j < j0 + F32_CHUNK; ++j) {
+        const float4 A = s_pos[j], B = s_nrm[j], C = s_den[j];
+        const float2 msx = make_float2(A.x, A.y), msy = make_float2(A.z, A.w);
+        const float2 nx = make_float2(B.x, B.y), ny = make_float2(B.z, B.w);
+        const float2 wx = make_float2(C.x, C.y), wy = make_float2(C.z, C.w);
+#pragma unroll
+        for (int p = 0; p < TP; ++p) {
+          const float2 rx = __fadd2_rn(PX[p], msx);
+          const float2 ry = __fadd2_rn(PY[p], msy);
+          const float2 rho2 = __ffma2_rn(rx, rx, __fmul2_rn(ry, ry));
+          const float2 rdn = __ffma2_rn(rx, nx, __fmul2_rn(ry, ny));
+          const float2 rds = __ffma2_rn(rx, wx, __fmul2_rn(ry, wy));
+          const float2 inv = make_float2(rcp_approx(rho2.x), rcp_approx(rho2.y));
+          const float2 c = __fmul2_rn(__fmul2_rn(rdn, rds), __fmul2_rn(inv, inv));
+          TX[p] = __ffma2_rn(c, rx, TX[p]);
+          TY[p] = __ffma2_rn(c, ry, TY[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < TP; ++p) {   // a select, not a product: an own-curve tile holds inf/NaN terms
+        two_sum_add2(HX[p], LX[p], make_float2(U0[p] ? TX[p].x : 0.f, U1[p] ? TX[p].y : 0.f));
+        two_sum_add2(HY[p], LY[p], make_float2(U0[p] ? TY[p].x : 0.f, U1[p] ? TY[p].y : 0.f));
+      }
     }
   }
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
     int i = i0 + q * NT;
-    if (i < N) partial[(size_t)split * N + i] = make_double2((double)hx[q] + (double)lx[q], (double)hy[q] + (double)ly[q]);
+    const int p = q >> 1;
+    const float hx = (q & 1) ? HX[p].y : HX[p].x, lx = (q & 1) ? LX[p].y : LX[p].x;
+    const float hy = (q & 1) ? HY[p].y : HY[p].x, ly = (q & 1) ? LY[p].y : LY[p].x;
+    if (i < N) partial[(size_t)split * N + i] = make_double2((double)hx + (double)lx, (double)hy + (double)ly);
   }
 }
 
@@ -666,7 +711,7 @@ k_pc_blocks(GeoDev G, float* __restrict__ B) {
 }
 
 // In-place Gauss-Jordan inversion with partial pivoting of a batch of m x m
-// FP32 matrices, one CTA per matrix.  Singular pivots set *bad.
+// FP32 matrices, one CTA per matrix.  A zero pivot sets bad[matrix].
 __global__ void __launch_bounds__(1024)
 k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
   extern __shared__ float gjs[];
@@ -700,7 +745,7 @@ k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
         int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
         if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
       }
-      if (tid == 0) { piv[k] = bi; if (!(best > 0.f)) atomicOr(bad, 1); }
+      if (tid == 0) { piv[k] = bi; if (!(best > 0.f)) bad[blockIdx.x] = 1; }
     }
     __syncthreads();
     const int p = piv[k];
@@ -742,6 +787,20 @@ k_gj_inv32(int m, float* __restrict__ B, int* __restrict__ bad) {
       }
     }
     __syncthreads();
+  }
+}
+
+// Replaces the inverse of every flagged (singular) block by the identity,
+// rows blockIdx.y * 8 .. + 7 of body blockIdx.x.
+__global__ void __launch_bounds__(256)
+k_pc_identity_if_bad(int m, const int* __restrict__ bad, float* __restrict__ B) {
+  const int b = blockIdx.x;
+  if (!bad[b]) return;
+  float* A = B + (size_t)b * m * m;
+  const int r0 = blockIdx.y * 8;
+  for (int e = threadIdx.x; e < 8 * m; e += blockDim.x) {
+    const int r = r0 + e / m, c = e % m;
+    if (r < m) A[(size_t)r * m + c] = r == c ? 1.f : 0.f;
   }
 }
 

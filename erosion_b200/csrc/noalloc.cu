@@ -111,11 +111,10 @@ struct Carve {
   }
 };
 
+// The status channel is per thread and lock-free (set_status), so recording
+// an outcome never waits for another thread's call into the library.
 int na_fail(int code, const char* msg) {
-  eb::State& s = eb::state();
-  std::lock_guard<std::mutex> lk(s.mu);
-  s.status = code;
-  s.err = msg;
+  eb::set_status(code, msg);
   return code;
 }
 
@@ -149,6 +148,16 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError();
       return na_fail(EROSION_NO_DEVICE, "erosion_matvec_noalloc: no CUDA device");
+    }
+    // This call shares the caller's stream and the runtime's per-thread error
+    // state: an error already pending from the caller's own work is reported
+    // (and left pending) instead of being consumed by the launch checks below.
+    {
+      const cudaError_t pending = cudaPeekAtLastError();
+      if (pending != cudaSuccess)
+        return na_fail(EROSION_CUDA_ERROR, (std::string("erosion_matvec_noalloc: a CUDA error was already pending "
+                                                        "before the call, nothing was launched: ") +
+                                            cudaGetErrorString(pending)).c_str());
     }
     int dev = 0;
     EB_CK(cudaGetDevice(&dev));
@@ -233,12 +242,11 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
     k_combine<<<nblk((long long)N * COMBINE_G, 256), 256, 0, st>>>(G, d_den, partial, nsplit, nullptr, nullptr, nullptr, sigdotn, selfsum,
                                             nslots, 1, d_vel);
     EB_LAUNCH_CHECK();
-    State& s = state();
-    std::lock_guard<std::mutex> lk(s.mu);
-    s.status = EROSION_OK;
-    s.err.clear();
+    set_status(EROSION_OK, "");
     return EROSION_OK;
   } catch (const Error& e) {
     return na_fail(e.code, e.what());
+  } catch (const std::exception& e) {
+    return na_fail(EROSION_CUDA_ERROR, e.what());
   }
 }

@@ -78,8 +78,7 @@ extern "C" double erosion_peak_tflops(int32_t precision) {
     cudaEventDestroy(b);
     return best;
   } catch (const Error& e) {
-    s.status = e.code;
-    s.err = e.what();
+    set_status(e.code, e.what());
     return -1.0;
   }
 }

@@ -2,6 +2,7 @@
 // C ABI entry points that replace the reference's libstokes.so.
 #include "state.h"
 #include "kernels.cuh"
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -13,6 +14,14 @@ State& state() {
 }
 
 long long g_launches = 0;
+
+thread_local int t_status = EROSION_OK;
+thread_local std::string t_err;
+
+void set_status(int code, const std::string& msg) {
+  t_status = code;
+  t_err = msg;
+}
 static int g_num_sms = 148;
 int eb_num_sms() { return g_num_sms; }
 
@@ -378,6 +387,7 @@ static void plan_far(State& s) {
 }
 
 void setup_problem(State& s, const Problem& in, const double* d_xx, const double* d_yy) {
+  const auto t_start = std::chrono::steady_clock::now();
   Problem pr = in;
   if (pr.nout < 8 || (pr.nout & 1)) throw Error(EROSION_BAD_INPUT, "nouter must be even and >= 8");
   if (pr.M < 0) throw Error(EROSION_BAD_INPUT, "nbods must be >= 0");
@@ -453,6 +463,15 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   plan_far(s);
   setup_preconditioner(s);
   s.geo_valid = true;
+  s.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  record_setup_stats(s);
+}
+
+void record_setup_stats(State& s) {
+  s.stats.precond_active = s.pc_active ? 1 : 0;
+  s.stats.precond_singular_blocks = s.pc_singular;
+  s.stats.ms_setup = s.setup_ms;
+  s.stats.ms_precond_setup = s.pc_setup_ms;
 }
 
 bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned) {
@@ -509,21 +528,35 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
 void setup_preconditioner(State& s) {
   const Problem& pr = s.pr;
   s.pc_active = false;
+  s.pc_singular = 0;
+  s.pc_setup_ms = 0.0;
   if (pr.P.precond != 1 || pr.M == 0) return;
   const int n = pr.n, m = 2 * n + 3;
   const GeoDev G = s.geo();
+  EB_CK(cudaEventRecord(s.et0, s.st));
   float* B = s.pcB.ensure((size_t)pr.M * m * m);
   k_pc_blocks<<<dim3(pr.M, m), 256, 0, s.st>>>(G, B);
   EB_LAUNCH_CHECK();
-  int* bad = s.pc_bad.ensure(1);
-  EB_CK(cudaMemsetAsync(bad, 0, sizeof(int), s.st));
+  int* bad = s.pc_bad.ensure(pr.M);
+  EB_CK(cudaMemsetAsync(bad, 0, sizeof(int) * pr.M, s.st));
   const size_t smem = 3 * (size_t)m * sizeof(float);
   if (smem > 48 * 1024) EB_CK(cudaFuncSetAttribute(k_gj_inv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
   EB_LAUNCH_CHECK();
-  int hbad = 0;
-  d2h(&hbad, bad, 1, s.st);
+  // a body whose block had a zero pivot gets the identity (left
+  // unpreconditioned); the other bodies keep their inverses
+  k_pc_identity_if_bad<<<dim3(pr.M, nblk(m, 8)), 256, 0, s.st>>>(m, bad, B);
+  EB_LAUNCH_CHECK();
+  EB_CK(cudaEventRecord(s.et1, s.st));
+  std::vector<int> hbad(pr.M);
+  d2h(hbad.data(), bad, pr.M, s.st);
   EB_CK(cudaStreamSynchronize(s.st));
+  {
+    float t = 0;
+    EB_CK(cudaEventElapsedTime(&t, s.et0, s.et1));
+    s.pc_setup_ms = t;
+  }
+  for (int b = 0; b < pr.M; ++b) s.pc_singular += hbad[b] != 0;
   s.pc_z.ensure(pr.ntot);
   s.pc_u.ensure(pr.ntot);
   {
@@ -532,7 +565,7 @@ void setup_preconditioner(State& s) {
   }
   s.pc_tw.ensure((size_t)s.pc_wsplit * pr.M * n);
   s.pc_ws32.ensure(pr.nout);
-  s.pc_active = hbad == 0;   // a singular block leaves the solve unpreconditioned
+  s.pc_active = s.pc_singular < pr.M;
 }
 
 void apply_preconditioner(State& s, const double* v, double* z) {
@@ -926,17 +959,14 @@ int guarded(F&& f) {
   try {
     ensure_init(s);
     int rc = f(s);
-    s.status = rc;
-    s.err = rc == EROSION_OK ? "" : (rc == EROSION_MAXITER ? "GMRES reached maxl before the tolerance"
-                                                            : (rc == EROSION_BREAKDOWN ? "GMRES stalled" : "error"));
+    set_status(rc, rc == EROSION_OK ? "" : (rc == EROSION_MAXITER ? "GMRES reached maxl before the tolerance"
+                                                            : (rc == EROSION_BREAKDOWN ? "GMRES stalled" : "error")));
     return rc;
   } catch (const Error& e) {
-    s.status = e.code;
-    s.err = e.what();
+    set_status(e.code, e.what());
     return e.code;
   } catch (const std::exception& e) {
-    s.status = EROSION_CUDA_ERROR;
-    s.err = e.what();
+    set_status(EROSION_CUDA_ERROR, e.what());
     return EROSION_CUDA_ERROR;
   }
 }
@@ -969,6 +999,7 @@ int solve_device_impl(State& s, double* d_den, bool x0_zero, int64_t* nits) {
     s.stats = erosion_solve_stats{};
     s.stats.guess_used = gu;
     for (int q = 0; q < 3; ++q) s.stats.guess_residual[q] = gr[q];
+    record_setup_stats(s);
   }
   EB_CK(cudaEventRecord(s.e0, s.st));
   double* rhs = s.d_rhs.ensure(pr.ntot);
@@ -1016,8 +1047,8 @@ void erosion_default_params(erosion_params* p) {
   p->true_residual = 0;
 }
 
-int erosion_last_status(void) { return state().status; }
-const char* erosion_last_error(void) { return state().err.c_str(); }
+int erosion_last_status(void) { return t_status; }
+const char* erosion_last_error(void) { return t_err.c_str(); }
 
 void erosion_get_solve_stats(erosion_solve_stats* out) { *out = state().stats; }
 
@@ -1149,8 +1180,7 @@ void* erosion_stream(void) {
   try {
     ensure_init(s);
   } catch (const Error& e) {
-    s.status = e.code;
-    s.err = e.what();
+    set_status(e.code, e.what());
     return nullptr;
   }
   return (void*)s.st;
@@ -1163,8 +1193,7 @@ int erosion_set_far_shape(int32_t kind, int32_t shape) {
   std::lock_guard<std::mutex> lk(s.mu);
   const int nsh = kind == 0 ? kNumFar64Shapes : kNumFar32Shapes;
   if ((kind != 0 && kind != 1) || shape < -1 || shape >= nsh) {
-    s.status = EROSION_BAD_INPUT;
-    s.err = "unknown far-field kernel kind or shape";
+    set_status(EROSION_BAD_INPUT, "unknown far-field kernel kind or shape");
     return EROSION_BAD_INPUT;
   }
   s.force_shape[kind] = shape;

@@ -103,8 +103,6 @@ struct Near {
 
 struct State {
   std::mutex mu;
-  int status = EROSION_OK;
-  std::string err;
   bool init = false;
   int device = -1;
   cudaStream_t st = nullptr;
@@ -152,7 +150,10 @@ struct State {
   DBuf<double> pc_z, pc_u;  // scratch vectors
   DBuf<double2> pc_tw;      // A_bw z_wall per body node
   DBuf<float2> pc_ws32;     // wall strengths of the coupling sum
-  DBuf<int> pc_bad;
+  DBuf<int> pc_bad;         // per body: 1 when its block had a zero pivot
+  int pc_singular = 0;      // bodies left unpreconditioned
+  double pc_setup_ms = 0.0; // device time of block assembly + inversion
+  double setup_ms = 0.0;    // host wall time of the last setup_problem
   int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32
 
   // work buffers
@@ -182,6 +183,10 @@ struct State {
 
 State& state();
 int eb_num_sms();
+// The outcome of the last entry-point call made by the calling thread,
+// read back by erosion_last_status / erosion_last_error.  Thread-local, so it
+// takes no lock and one thread's call never overwrites another's outcome.
+void set_status(int code, const std::string& msg);
 void ensure_init(State& s);
 
 // Geometry + near lists + far-field tiles for (xx, yy) already on the device.
@@ -209,6 +214,8 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
 bool lw_guess_current(State& s, double* d_den);
 // Builds (or disables) the block preconditioner for the current geometry.
 void setup_preconditioner(State& s);
+// Copies the last set-up's figures (time, preconditioner state) into s.stats.
+void record_setup_stats(State& s);
 // z = P^{-1} v (device vectors of length ntot).
 void apply_preconditioner(State& s, const double* v, double* z);
 double device_norm(State& s, const double* d_v, long long n);

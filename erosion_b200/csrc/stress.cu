@@ -576,16 +576,13 @@ int guarded2(F&& f) {
   try {
     ensure_init(s);
     int rc = f(s);
-    s.status = rc;
-    s.err = "";
+    set_status(rc, "");
     return rc;
   } catch (const Error& e) {
-    s.status = e.code;
-    s.err = e.what();
+    set_status(e.code, e.what());
     return e.code;
   } catch (const std::exception& e) {
-    s.status = EROSION_CUDA_ERROR;
-    s.err = e.what();
+    set_status(EROSION_CUDA_ERROR, e.what());
     return EROSION_CUDA_ERROR;
   }
 }

@@ -95,6 +95,49 @@ k_tl_atau(int n, const double* __restrict__ tau, const double* __restrict__ gker
   if (threadIdx.x == 0) matau[b] = s / n;
 }
 
+// xyrot (DensityStress.jl:40): (x, y) -> (-y, x), in place.
+__global__ void k_tl_xyrot(long long nb, double* __restrict__ xx, double* __restrict__ yy) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const double x = xx[i], y = yy[i];
+  xx[i] = -y;
+  yy[i] = x;
+}
+
+// drag (PostProcess.jl:131-162) per body: the pressure and viscous parts
+//   pdrag = sum_k p_k n_k ds,  vdrag = sum_k tau_k s_k ds,  ds = L / n,
+// with the tangent s = (cos th, sin th), rotated (-sin th, cos th) for the
+// rotated flow, and the inward normal n = (-s_y, s_x) of getns
+// (PostProcess.jl:23-33).  out[4 b + (0..3)] = pdragx, pdragy, vdragx, vdragy.
+__global__ void __launch_bounds__(TL_NT)
+k_tl_drag(int n, const double* __restrict__ th, const double* __restrict__ len, const double* __restrict__ press,
+          const double* __restrict__ tau, int rotation, double* __restrict__ out) {
+  __shared__ double red[32];
+  const int b = blockIdx.x;
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const size_t i = (size_t)b * n + j;
+    const double c = cos(th[i]), sn = sin(th[i]);
+    const double sx = rotation ? -sn : c, sy = rotation ? c : sn;
+    const double nx = -sy, ny = sx;
+    a0 += press[i] * nx;
+    a1 += press[i] * ny;
+    a2 += tau[i] * sx;
+    a3 += tau[i] * sy;
+  }
+  const double ds = len[b] / n;
+  a0 = block_sum<TL_NT>(a0, red);
+  a1 = block_sum<TL_NT>(a1, red);
+  a2 = block_sum<TL_NT>(a2, red);
+  a3 = block_sum<TL_NT>(a3, red);
+  if (threadIdx.x == 0) {
+    out[4 * b] = a0 * ds;
+    out[4 * b + 1] = a1 * ds;
+    out[4 * b + 2] = a2 * ds;
+    out[4 * b + 3] = a3 * ds;
+  }
+}
+
 // getderivs for one body per CTA (TimeStepping.jl:42-83).
 __global__ void __launch_bounds__(TL_NT)
 k_tl_derivs(int n, const double* __restrict__ th, const double* __restrict__ len, const double* __restrict__ atau,
@@ -340,6 +383,10 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   Problem pr = base;
   pr.M = M;
   setup_problem(s, pr, T.xx.p, T.yy.p);
+  T.stats.ms_setup += s.setup_ms;
+  T.stats.ms_precond_setup += s.pc_setup_ms;
+  T.stats.precond_active[k] = s.pc_active ? 1 : 0;
+  T.stats.precond_singular_blocks[k] = s.pc_singular;
   const long long ntot = s.pr.ntot;
   double* den = T.den[k].ensure(ntot);
   const bool have_prev = sp.warm_start && T.den_ntot[k] == ntot;
@@ -351,7 +398,10 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   T.stats.guess_residual[k] = s.stats.guess_used >= 0 ? s.stats.guess_residual[s.stats.guess_used] : -1;
   long long it = 0;
   double est = 0;
+  const long long mv0 = s.stats.matvecs, mv32 = s.stats.matvecs_fp32;
   int rc = gmres_solve(s, rhs, den, zero, s.pr.P.maxl, s.pr.P.tol, &it, &est);
+  T.stats.matvecs[k] = s.stats.matvecs - mv0;
+  T.stats.matvecs_fp32[k] = s.stats.matvecs_fp32 - mv32;
   if (rc == EROSION_BREAKDOWN) throw Error(EROSION_BREAKDOWN, "GMRES stalled inside the time step");
   T.den_ntot[k] = ntot;
   *iters = it;
@@ -543,16 +593,13 @@ int guarded3(F&& f) {
   try {
     ensure_init(s);
     int rc = f(s);
-    s.status = rc;
-    s.err = "";
+    set_status(rc, "");
     return rc;
   } catch (const Error& e) {
-    s.status = e.code;
-    s.err = e.what();
+    set_status(e.code, e.what());
     return e.code;
   } catch (const std::exception& e) {
-    s.status = EROSION_CUDA_ERROR;
-    s.err = e.what();
+    set_status(EROSION_CUDA_ERROR, e.what());
     return EROSION_CUDA_ERROR;
   }
 }
@@ -614,6 +661,77 @@ int erosion_rk2_step(const erosion_params* p, const erosion_step_params* sp, int
     EB_CK(cudaStreamSynchronize(s.st));
     *nbods = Mo;
     return rc;
+  });
+}
+
+int erosion_drag(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* theta,
+                 const double* len, const double* xsm, const double* ysm, const double* density, int32_t rotation,
+                 double sigma, double* drag, double* drag_bodies, double* tau_all, double* atau_all,
+                 double* press_all) {
+  return guarded3([&](State& s) {
+    const int n = (int)npts, M = (int)nbods;
+    if (n < 4 || (n & 1) || M <= 0 || nouter < 8 || (nouter & 1) || nouter > (1 << 26) || n > (1 << 20))
+      throw Error(EROSION_BAD_INPUT, "erosion_drag: npts and nouter must be even, nbods > 0");
+    if (!theta || !len || !xsm || !ysm || !density || !drag) throw Error(EROSION_BAD_INPUT, "erosion_drag: null array");
+    if (!(sigma > 0)) throw Error(EROSION_BAD_INPUT, "erosion_drag: sigma must be positive");
+    Problem pr = base_problem(p, npts, nouter);
+    pr.M = M;
+    pr.P.precond = 0;   // no solve here: skip the preconditioner's set-up
+    pr.P.learned_guess = 0;
+    TL& T = tl();
+    ensure_spectral(s, n);
+    tl_tables(s, T, n, sigma);
+    T.flag.ensure(1);
+    EB_CK(cudaMemsetAsync(T.flag.p, 0, sizeof(int), s.st));
+    const size_t nb = (size_t)M * n;
+    static DBuf<double> buf;
+    double* b = buf.ensure(8 * nb + 8 * (size_t)M + 4);
+    double* dth = b;
+    double* dl = dth + nb;
+    double* dxs = dl + M;
+    double* dys = dxs + M;
+    double* dx = dys + M;
+    double* dy = dx + nb;
+    double* dtau = dy + nb;
+    double* datau = dtau + nb;
+    double* dp = datau + nb;
+    double* dmat = dp + nb;
+    double* dper = dmat + M;   // 4 M
+    h2d(dth, theta, nb, s.st);
+    h2d(dl, len, M, s.st);
+    h2d(dxs, xsm, M, s.st);
+    h2d(dys, ysm, M, s.st);
+    k_tl_getxy<<<M, TL_NT, 3 * n * sizeof(double), s.st>>>(n, dth, dl, dxs, dys, T.iker.p, dx, dy, T.flag.p);
+    EB_LAUNCH_CHECK();
+    if (rotation) {
+      k_tl_xyrot<<<nblk((long long)nb, 256), 256, 0, s.st>>>((long long)nb, dx, dy);
+      EB_LAUNCH_CHECK();
+    }
+    setup_problem(s, pr, dx, dy);
+    const long long ntot = s.pr.ntot;
+    double* dden = T.tmp.ensure(std::max<size_t>(ntot, nb));
+    h2d(dden, density, ntot, s.st);
+    shear_stress(s, dden, dtau, nullptr);
+    body_pressure(s, dden, dp);
+    k_tl_atau<<<M, TL_NT, 2 * n * sizeof(double), s.st>>>(n, dtau, T.gker.p, datau, dmat);
+    EB_LAUNCH_CHECK();
+    k_tl_drag<<<M, TL_NT, 0, s.st>>>(n, dth, dl, dp, dtau, rotation ? 1 : 0, dper);
+    EB_LAUNCH_CHECK();
+    std::vector<double> per(4 * (size_t)M);
+    d2h(per.data(), dper, 4 * (size_t)M, s.st);
+    if (tau_all) d2h(tau_all, dtau, nb, s.st);
+    if (atau_all) d2h(atau_all, datau, nb, s.st);
+    if (press_all) d2h(press_all, dp, nb, s.st);
+    int flag = 0;
+    d2h(&flag, T.flag.p, 1, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    if (flag) throw Error(EROSION_BAD_INPUT, "erosion_drag: a body length is not positive");
+    // totals in body order, as the reference's loop accumulates them
+    for (int q = 0; q < 4; ++q) drag[q] = 0.0;
+    for (int bb = 0; bb < M; ++bb)
+      for (int q = 0; q < 4; ++q) drag[q] += per[4 * (size_t)bb + q];
+    if (drag_bodies) std::copy(per.begin(), per.end(), drag_bodies);
+    return EROSION_OK;
   });
 }
 

@@ -292,3 +292,41 @@ def rungekutta2(thld0: ThLenDenType, params: ParamSet) -> tuple[ThLenDenType, di
     stats = st.as_dict()
     stats["deleted"] = deleted[:M - Mn].tolist()
     return out, stats
+
+
+@dataclasses.dataclass
+class DragData:
+    """PostProcess.jl:126-129."""
+    pdragx: float
+    pdragy: float
+    vdragx: float
+    vdragy: float
+    umax: float
+    tau_all: np.ndarray     # (npts, nbods)
+    atau_all: np.ndarray    # (npts, nbods)
+    press_all: np.ndarray   # (npts, nbods)
+
+
+def drag(thlenden: ThLenDenType, params: ParamSet, rotation: bool = False) -> DragData:
+    """drag (PostProcess.jl:131-162) through erosion_drag: the pressure and
+    viscous drag summed over all bodies (density solved and cached first, as
+    compute_stress does), with the unsmoothed shear stress, its smoothed
+    absolute value and the pressure on every node (umax = 1 in all of them;
+    the reported umax follows params.fixpdrop as getumax does)."""
+    compute_density_(thlenden, params, rotation=rotation)
+    L = _lib.load()
+    M = len(thlenden.thlenvec)
+    n = params.npts
+    th, ln, xs, ys = pack_state(thlenden)
+    den = np.ascontiguousarray(thlenden.denrot if rotation else thlenden.density, dtype=np.float64)
+    out = np.zeros(4)
+    tau = np.zeros(M * n)
+    atau = np.zeros(M * n)
+    press = np.zeros(M * n)
+    p = params.erosion_params()
+    check(L.erosion_drag(ctypes.byref(p), n, M, params.nouter, ptr(th), ptr(ln), ptr(xs), ptr(ys), ptr(den),
+                         1 if rotation else 0, params.sigma, ptr(out), None, ptr(tau), ptr(atau), ptr(press)))
+    umax = getumax(thlenden, params, params.fixpdrop)
+    shape = lambda a: a.reshape(M, n).T
+    return DragData(float(out[0]), float(out[1]), float(out[2]), float(out[3]), umax, shape(tau), shape(atau),
+                    shape(press))

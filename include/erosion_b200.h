@@ -70,7 +70,9 @@ void computeqoitargets_(const int64_t* npts, const int64_t* nbods, const int64_t
                         const double* xtar, const double* ytar, double* utar,
                         double* vtar, double* ptar, double* vortar);
 
-/* Outcome of the last call on this process (EROSION_* code) and a message. */
+/* Outcome (EROSION_* code) and message of the last entry-point call made by
+ * the calling thread; each thread has its own.  The string stays valid until
+ * that thread's next call into the library. */
 int erosion_last_status(void);
 const char* erosion_last_error(void);
 
@@ -142,6 +144,15 @@ typedef struct {
                                far-field launches                                  */
   int64_t farw_launches;    /* their count                                         */
   int64_t farw_pairs;       /* wall-source pairs per such launch                   */
+  int64_t precond_active;   /* 1: the block preconditioner was applied             */
+  int64_t precond_singular_blocks; /* bodies whose FP32 block had a zero pivot; each
+                               such body is left unpreconditioned (identity block)
+                               while the others keep theirs                        */
+  double ms_setup;          /* host wall time of the last geometry set-up: node
+                               geometry, near lists, far-field tiles, launch shapes
+                               and the preconditioner                              */
+  double ms_precond_setup;  /* device time of the preconditioner's block assembly
+                               and inversion within that set-up                    */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
@@ -209,7 +220,10 @@ int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t
  * device address; make it before capturing any stream.  Calls share the
  * array: calls whose kernels overlap on the GPU race and must be ordered by
  * the caller.  Inputs are not checked for finiteness or for bodies inside the
- * wall. */
+ * wall.  A CUDA error already pending on the calling thread when the call
+ * starts is reported as EROSION_CUDA_ERROR (nothing is launched) and left
+ * pending for the caller.  The call takes no library lock: it never waits on
+ * the host for another thread's call into the library. */
 int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                            const double* d_xx, const double* d_yy, const double* d_den, double* d_vel,
                            void* stream);
@@ -301,6 +315,16 @@ typedef struct {
   int64_t guess_used[2];        /* initial guess per stage: 0 zero, 1 previous,
                                    2 learned                                  */
   double guess_residual[2];     /* its relative residual ||b - A x0||/||b||   */
+  double ms_setup;              /* host wall time of the two geometry set-ups
+                                   (included in ms_solve)                     */
+  double ms_precond_setup;      /* device time of the two preconditioner
+                                   set-ups (included in ms_setup)             */
+  int64_t precond_active[2];    /* per stage: 1 when the block preconditioner
+                                   was applied                                */
+  int64_t precond_singular_blocks[2]; /* per stage: bodies left
+                                   unpreconditioned (zero pivot)              */
+  int64_t matvecs[2];           /* per stage: operator applications           */
+  int64_t matvecs_fp32[2];      /* per stage: of which with the FP32 far field */
 } erosion_step_stats;
 
 /* One RK2 step of the theta-L state, host arrays, in place:
@@ -317,6 +341,25 @@ int erosion_rk2_step_device(const erosion_params* p, const erosion_step_params* 
                             double* d_xsm, double* d_ysm, double* t, int64_t* deleted);
 
 void erosion_get_step_stats(erosion_step_stats* s);
+
+/* Drag on the bodies of a theta-L state: replaces drag (PostProcess.jl:131-162)
+ * with the shear stress and pressure it calls (compute_stress,
+ * compute_pressure: computeshearstress_/computepressure_ semantics with
+ * fixpdrop off, i.e. umax = 1).  Host arrays: theta[nbods*npts],
+ * len/xsm/ysm[nbods]; density is the solved density of that state (with
+ * rotation != 0: of the rotated problem, the bodies turned by xyrot,
+ * DensityStress.jl:40).  Per body, ds = L/npts, tangent s = (cos th, sin th)
+ * (rotated: (-sin th, cos th)) and inward normal n = (-s_y, s_x) (getns,
+ * PostProcess.jl:23-33):
+ *   pdrag = sum p n ds,   vdrag = sum tau s ds.
+ * drag[4] receives the totals (pdragx, pdragy, vdragx, vdragy) summed in body
+ * order; drag_bodies[4*nbods] (optional) the per-body parts; tau_all,
+ * atau_all (gaussfilter(|tau|, sigma)) and press_all [npts*nbods] (optional)
+ * the DragData arrays. */
+int erosion_drag(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter, const double* theta,
+                 const double* len, const double* xsm, const double* ysm, const double* density, int32_t rotation,
+                 double sigma, double* drag, double* drag_bodies, double* tau_all, double* atau_all,
+                 double* press_all);
 
 /* Node coordinates of theta-L bodies (getxy, ThetaLen.jl:92-101), host arrays. */
 int erosion_getxy(int64_t npts, int64_t nbods, const double* theta, const double* len,

@@ -44,6 +44,7 @@ class Oracle:
         L.oracle_rhs.argtypes = [c_int64] * 5 + [PD, PD, PD, PD]
         L.oracle_geometry.argtypes = [c_int64] * 3 + [PD] * 15
         L.oracle_shear_stress.argtypes = [c_int64] * 3 + [PD, PD, PD, c_int64, PD, PD, PD]
+        L.oracle_shear_stress_bodies.argtypes = [c_int64] * 3 + [PD, PD, PD, c_int64, PD, ctypes.c_void_p, PD, PD]
         L.oracle_qoi_targets.argtypes = [c_int64] * 4 + [PD, PD, PD, c_int64, PD, PD, PD, PD, PD, PD, PD]
         L.oracle_pressure.argtypes = [c_int64] * 3 + [PD, PD, PD, PD, PD]
         L.oracle_near_wall.restype = c_int64
@@ -97,12 +98,21 @@ class Oracle:
                                                     "px0", "py0", "cur0", "speed0")])
         return a
 
-    def shear_stress(self, g, den, ibary=1):
+    def shear_stress(self, g, den, ibary=1, bodies=None):
+        """(tau, E) on every body, or, with bodies (indices), on those target
+        bodies only (from every source curve; the other entries are zero)."""
         tau = np.zeros(g.n * g.M)
         E = np.zeros(3 * g.n * g.M)
         den = np.ascontiguousarray(den, dtype=np.float64)
-        self.L.oracle_shear_stress(g.n, g.M, g.nout, _p(g.xx), _p(g.yy), _p(den), ibary, _p(_wall(g.wall)),
-                                   _p(tau), _p(E))
+        if bodies is None:
+            self.L.oracle_shear_stress(g.n, g.M, g.nout, _p(g.xx), _p(g.yy), _p(den), ibary, _p(_wall(g.wall)),
+                                       _p(tau), _p(E))
+        else:
+            sel = np.zeros(max(g.M, 1), np.uint8)
+            sel[np.asarray(bodies, int)] = 1
+            self.L.oracle_shear_stress_bodies(g.n, g.M, g.nout, _p(g.xx), _p(g.yy), _p(den), ibary,
+                                              _p(_wall(g.wall)), sel.ctypes.data_as(ctypes.c_void_p), _p(tau),
+                                              _p(E))
         return tau, E.reshape(3, -1)
 
     def qoi_targets(self, g, den, xt, yt, ibary=1):

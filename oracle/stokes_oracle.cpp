@@ -818,8 +818,12 @@ void self_odd_even(const Geo& g, int s, const double* dx, const double* dy, doub
   pass(1, 0);   // Fortran k = 2,4,.. with sources j = 1,3,..  (:2791-2833)
 }
 
-void deformation(const Geo& g, const double* den, int ib, double* E11, double* E12, double* E22) {
+// tsel (optional, M flags): evaluate only the target bodies whose flag is set,
+// with every source curve (the other bodies' entries are left at zero).
+void deformation(const Geo& g, const double* den, int ib, double* E11, double* E12, double* E22,
+                 const unsigned char* tsel = nullptr) {
   const int nout = g.nout, n = g.n, M = g.M;
+  auto want = [&](int b) { return tsel == nullptr || tsel[b] != 0; };
   size_t nb = size_t(n) * M;
   std::fill(E11, E11 + nb, 0.0); std::fill(E12, E12 + nb, 0.0); std::fill(E22, E22 + nb, 0.0);
   std::vector<double> wdx(nout), wdy(nout);
@@ -827,6 +831,7 @@ void deformation(const Geo& g, const double* den, int ib, double* E11, double* E
   DLPOut o;
   if (ib == 1) {
     for (int t = 0; t < M; ++t) {   // :2707-2727
+      if (!want(t)) continue;
       stokes_dlp(false, nout, g.xo.data(), g.yo.data(), wdx.data(), wdy.data(), g.px0.data(), g.py0.data(), n,
                  &g.x[t * n], &g.y[t * n], 2, o);
       for (int k = 0; k < n; ++k) {
@@ -838,6 +843,7 @@ void deformation(const Geo& g, const double* den, int ib, double* E11, double* E
   } else {   // :2350-2384
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < int(nb); ++i) {
+      if (!want(i / n)) continue;
       double e11 = 0, e12 = 0, e22 = 0;
       for (int j = 0; j < nout; ++j) {
         double rx = g.x[i] - g.xo[j], ry = g.y[i] - g.yo[j];
@@ -858,10 +864,10 @@ void deformation(const Geo& g, const double* den, int ib, double* E11, double* E
   for (int s = 0; s < M; ++s) {
     std::vector<double> dx(n), dy(n);
     for (int k = 0; k < n; ++k) { dx[k] = den[ibx(g, s, k)]; dy[k] = den[iby(g, s, k)]; }
-    self_odd_even(g, s, dx.data(), dy.data(), &E11[s * n], &E12[s * n], &E22[s * n]);
+    if (want(s)) self_odd_even(g, s, dx.data(), dy.data(), &E11[s * n], &E12[s * n], &E22[s * n]);
     const double* xs = &g.x[s * n]; const double* ys = &g.y[s * n];
     for (int t = 0; t < M; ++t) {
-      if (t == s) continue;
+      if (t == s || !want(t)) continue;
       if (ib == 1) {   // :2893-2925
         stokes_dlp(true, n, xs, ys, dx.data(), dy.data(), &g.px[s * n], &g.py[s * n], n, &g.x[t * n], &g.y[t * n], 2, o);
         for (int k = 0; k < n; ++k) {
@@ -897,6 +903,7 @@ void deformation(const Geo& g, const double* den, int ib, double* E11, double* E
   // jump (:2933-2958)
   std::vector<cd> zd(n);
   for (int b = 0; b < M; ++b) {
+    if (!want(b)) continue;
     for (int k = 0; k < n; ++k) zd[k] = cd(den[ibx(g, b, k)], den[iby(g, b, k)]);
     fourier_diff(n, zd.data());
     for (int k = 0; k < n; ++k) {
@@ -914,6 +921,7 @@ void deformation(const Geo& g, const double* den, int ib, double* E11, double* E
   for (int b = 0; b < M; ++b) {
     double s1 = den[ic(g, b, 0)], s2 = den[ic(g, b, 1)], rot = den[ic(g, b, 2)];
     for (size_t i = 0; i < nb; ++i) {
+      if (!want(int(i / n))) continue;
       double rx = g.x[i] - g.cx[b], ry = g.y[i] - g.cy[b];
       double rho2 = rx * rx + ry * ry, rd = rx * s1 + ry * s2;
       E11[i] += 0.5 / TWOPI * (rd / rho2 - 2 * rx * rx * rd / rho2 / rho2);
@@ -1225,13 +1233,25 @@ int64_t oracle_stokessolver(int64_t n, int64_t M, int64_t nout, int64_t ifmm, in
 
 // computeShearStress (stokesSolver.f:3002-3096).  E (3*n*M, optional) receives
 // E11, E12, E22.
+void oracle_shear_stress_bodies(int64_t n, int64_t M, int64_t nout, const double* xx, const double* yy,
+                                const double* density, int64_t ibary, const double* wallp,
+                                const unsigned char* tsel, double* tau, double* E);
+
 void oracle_shear_stress(int64_t n, int64_t M, int64_t nout, const double* xx, const double* yy, const double* density,
                          int64_t ibary, const double* wallp, double* tau, double* E) {
+  oracle_shear_stress_bodies(n, M, nout, xx, yy, density, ibary, wallp, nullptr, tau, E);
+}
+
+// The shear stress on the target bodies flagged in tsel (M bytes; NULL = all)
+// from every source curve; the other bodies' entries are zero.
+void oracle_shear_stress_bodies(int64_t n, int64_t M, int64_t nout, const double* xx, const double* yy,
+                                const double* density, int64_t ibary, const double* wallp,
+                                const unsigned char* tsel, double* tau, double* E) {
   Geo g;
   build_geo(g, int(n), int(M), int(nout), xx, yy, wall_from(wallp));
   size_t nb = size_t(n) * M;
   std::vector<double> e11(nb), e12(nb), e22(nb);
-  deformation(g, density, ibary == 1 ? 1 : 0, e11.data(), e12.data(), e22.data());
+  deformation(g, density, ibary == 1 ? 1 : 0, e11.data(), e12.data(), e22.data(), tsel);
   shear_from_E(g, e11.data(), e12.data(), e22.data(), tau);
   if (E) {
     std::copy(e11.begin(), e11.end(), E);

@@ -177,3 +177,47 @@ class ThetaLenOracle:
         thld05 = self.timestep(thld0, thld0, 0.5 * dt, 0.5 * dt)
         thld1 = self.timestep(thld0, thld05, dt, 0.5 * dt)
         return thld1
+
+
+# --- PostProcess.jl: getns, drag ------------------------------------------------
+def getns(theta, rotation=False):
+    """PostProcess.jl:23-33: CCW tangent (rotated for the rotated flow) and the
+    inward normal."""
+    if not rotation:
+        sx, sy = np.cos(theta), np.sin(theta)
+    else:
+        sx, sy = -np.sin(theta), np.cos(theta)
+    return sx, sy, -sy, sx
+
+
+def drag(oracle, bodies, den, nout, wall, ibc, sigma, rotation=False):
+    """drag (PostProcess.jl:131-162) for a solved density of the state
+    `bodies` (of the rotated problem when rotation): the shear stress and the
+    pressure on every node from the C++ oracle (computeShearStress,
+    computePressure semantics, umax = 1), per body
+    pdrag = sum p n ds, vdrag = sum tau s ds with ds = L/npts, summed in body
+    order.  Returns (pdragx, pdragy, vdragx, vdragy), tau_all, atau_all,
+    press_all (arrays (npts, nbods))."""
+    from erosion_b200.geometry import Geometry
+    xs, ys = zip(*[getxy(b) for b in bodies])
+    xv, yv = np.concatenate(xs), np.concatenate(ys)
+    if rotation:   # xyrot, DensityStress.jl:40
+        xv, yv = -yv, xv
+    n, M = len(bodies[0].theta), len(bodies)
+    g = Geometry(n, nout, np.ascontiguousarray(xv), np.ascontiguousarray(yv), wall, ibc, np.zeros(M),
+                 np.zeros((M, 2)))
+    tau, _ = oracle.shear_stress(g, den)
+    press = oracle.pressure(g, den)
+    tau = tau.reshape(M, n)
+    press = press.reshape(M, n)
+    pdx = pdy = vdx = vdy = 0.0
+    atau = np.zeros((M, n))
+    for b in range(M):
+        atau[b] = gaussfilter(np.abs(tau[b]), sigma)
+        sx, sy, nx, ny = getns(bodies[b].theta, rotation)
+        ds = bodies[b].len / n
+        pdx += np.dot(press[b], nx) * ds
+        pdy += np.dot(press[b], ny) * ds
+        vdx += np.dot(tau[b], sx) * ds
+        vdy += np.dot(tau[b], sy) * ds
+    return (pdx, pdy, vdx, vdy), tau.T, atau.T, press.T

@@ -243,3 +243,24 @@ def test_mlp_oracle_gradient_by_finite_differences(monkeypatch):
         p2[i] -= h
         fd = (mlp_oracle.loss_and_grad(p1, x, y)[0] - mlp_oracle.loss_and_grad(p2, x, y)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
+
+
+def test_drag_of_a_centred_circle_is_symmetric(oracle):
+    """drag (PostProcess.jl:131-162) restated in the oracle: a circle at the
+    centre of the reference channel in uniform flow feels drag along the flow
+    only (up-down symmetry: the y parts vanish), with positive pressure and
+    viscous parts; the circle is invariant under the 90-degree turn of the
+    rotated flow, so the rotated problem gives the same numbers."""
+    from oracle import thetalen_oracle as TO
+    b = TO.circ2thlen(64, 0.3, 0.0, 0.0)
+    x, y = TO.getxy(b)
+    g = G.Geometry(64, 256, x, y, G.REFERENCE_WALL, 1, np.array([0.3]), np.array([[0.0, 0.0]]))
+    den, _, _, _ = oracle.solve(g, tol=1e-12)
+    (pdx, pdy, vdx, vdy), tau, atau, press = TO.drag(oracle, [b], den, 256, G.REFERENCE_WALL, 1, 10 / 64)
+    assert pdx > 0 and vdx > 0
+    assert abs(pdy) < 1e-10 * pdx and abs(vdy) < 1e-10 * vdx
+    assert tau.shape == atau.shape == press.shape == (64, 1)
+    gr = G.Geometry(64, 256, -y, x, G.REFERENCE_WALL, 1, np.array([0.3]), np.array([[0.0, 0.0]]))
+    denr, _, _, _ = oracle.solve(gr, tol=1e-12)
+    rot = TO.drag(oracle, [b], denr, 256, G.REFERENCE_WALL, 1, 10 / 64, rotation=True)[0]
+    assert np.allclose(rot, (pdx, pdy, vdx, vdy), rtol=1e-9, atol=1e-9 * pdx)

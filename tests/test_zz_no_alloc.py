@@ -101,3 +101,44 @@ def test_noalloc_at_the_largest_channel_size_that_fits(lib):
     assert call_noalloc(lib, g, d_xx, d_yy, d_den, d_vel, stream) == _lib.EROSION_OK
     torch.cuda.synchronize()
     assert rel(d_vel.cpu().numpy(), want) < MATVEC_RTOL
+
+
+def test_noalloc_wall_only_channel(lib):
+    """nbods = 0: the wall alone (the body pointers may be null)."""
+    torch = pytest.importorskip("torch")
+    stream = torch.cuda.current_stream()
+    g = G.custom(64, 1024, [], [], wall=G.CHANNEL_WALL, ibc=0)
+    den = np.random.default_rng(13).standard_normal(g.ntot)
+    want = stokes.matvec(g, den, ibary=0, precision=0)
+    d_den = torch.tensor(den, dtype=torch.float64, device="cuda")
+    d_vel = torch.full((g.ntot,), float("nan"), dtype=torch.float64, device="cuda")
+    p = stokes.params_for(g, ibary=0)
+    for _ in range(2):
+        rc = lib.erosion_matvec_noalloc(ctypes.byref(p), g.n, 0, g.nout, None, None, d_den.data_ptr(),
+                                        d_vel.data_ptr(), stream.cuda_stream)
+        assert rc == _lib.EROSION_OK
+        torch.cuda.synchronize()
+        got = d_vel.cpu().numpy()
+        assert np.isfinite(got).all() and rel(got, want) < MATVEC_RTOL
+
+
+def test_noalloc_at_the_node_limit(lib):
+    """The largest accepted layout: nouter = 4096 and npts = 512 with 56 bodies
+    (4096 + 56 x 512 = 32,768 nodes), which leaves the least room for the
+    split-K partial sums; then a small call again."""
+    torch = pytest.importorskip("torch")
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(17)
+    n, nout, M = 512, 4096, 56
+    radii, cs = G.pack(M, 0.03, 0.05, G.CHANNEL_WALL, lambda r: 4 * 2 * np.pi * r / n, rng)
+    g = G.custom(n, nout, radii, cs, wall=G.CHANNEL_WALL, ibc=0)
+    assert g.N == 32768
+    small = G.workload("ref-small")
+    for geo, seed in ((g, 19), (small, 23), (g, 29)):
+        den = np.random.default_rng(seed).standard_normal(geo.ntot)
+        want = stokes.matvec(geo, den, ibary=0, precision=0)
+        d_xx, d_yy, d_den, d_vel = device_inputs(torch, geo, den)
+        assert call_noalloc(lib, geo, d_xx, d_yy, d_den, d_vel, stream) == _lib.EROSION_OK
+        torch.cuda.synchronize()
+        got = d_vel.cpu().numpy()
+        assert np.isfinite(got).all() and rel(got, want) < MATVEC_RTOL
