@@ -54,7 +54,10 @@ class ErosionParams(ctypes.Structure):
         ("true_residual", c_int32),
         ("precond", c_int32),
         ("learned_guess", c_int32),
-        ("reserved", c_int32 * 4),
+        ("fast_fp64", c_int32),
+        ("precond_refresh", c_int32),
+        ("stress_all_bary", c_int32),
+        ("reserved", c_int32 * 1),
         ("relax_tol", c_double),
     ]
 
@@ -90,6 +93,8 @@ class SolveStats(ctypes.Structure):
         ("precond_singular_blocks", c_int64),
         ("ms_setup", c_double),
         ("ms_precond_setup", c_double),
+        ("ms_far64f", c_double),
+        ("far64f_launches", c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -181,6 +186,8 @@ SIGNATURES = {
     "erosion_drag": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PD, PD, c_int32,
                              c_double, PD, PD, PD, PD, PD]),
     "erosion_stream": (ctypes.c_void_p, []),
+    "erosion_get_step_density": (c_int, [c_int32, PD, c_int64]),
+    "erosion_lw_dims": (c_int, [ctypes.POINTER(c_int32)] * 3),
     "erosion_lw_features": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32]),
     "erosion_lw_encode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PF32]),
     "erosion_lw_decode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32, PD]),
@@ -267,19 +274,22 @@ def solve_stats() -> dict:
     return s.as_dict()
 
 
+RCP_LABELS = {0: "div", 1: "f32est+2nr", 2: "f32est+1nr", 3: "f64est+2nr", 4: "f64est+1nr"}
+
+
 def far_shapes() -> dict:
     """The far-field launch shapes in use and the autotuner's timings."""
     lib = load()
-    shape = (c_int32 * 2)()
-    desc = (c_int32 * 24)()
-    ms = (ctypes.c_float * 16)()
-    num = (c_int32 * 2)()
+    shape = (c_int32 * 3)()
+    desc = (c_int32 * 36)()
+    ms = (ctypes.c_float * 24)()
+    num = (c_int32 * 3)()
     lib.erosion_get_far_shapes(shape, desc, ms, num)
     out = {}
-    for kind, name in ((0, "fp64"), (1, "fp32")):
+    for kind, name in ((0, "fp64"), (1, "fp32"), (2, "fp64_fast")):
         cands = [tuple(desc[12 * kind + 3 * i: 12 * kind + 3 * i + 3]) for i in range(num[kind])]
-        if kind == 0:
-            label = lambda c: f"{c[0]}x{c[1]}" + ("-newton" if c[2] else "")
+        if kind != 1:
+            label = lambda c: f"{c[0]}x{c[1]}-{RCP_LABELS.get(c[2], c[2])}"
         else:
             label = lambda c: f"{c[0]}x{c[1]}-unroll{c[2]}"
         out[name] = {"shape": label(cands[shape[kind]]), "index": shape[kind],

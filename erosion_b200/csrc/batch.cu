@@ -62,7 +62,7 @@ struct Batch {
   cudaEvent_t ev_far = nullptr, ev_start = nullptr;
   DBuf<FarJob64> jobs64;
   DBuf<FarJob32> jobs32;
-  int shape64 = 1, shape32 = 0;   // indices into kFar64Shapes / kFar32Shapes
+  int shape64 = 0, shape32 = 0;   // indices into kFar64Shapes / kFar32Shapes
   double* pinned = nullptr;
   size_t pinned_cap = 0;
   erosion_batch_stats stats{};
@@ -207,10 +207,10 @@ void launch_batch64(Batch& B, int shape, int njobs, long long items, cudaStream_
     break;                                                                                             \
   }
   switch (shape) {
-    EB_B64(0, 256, 2, 0)
-    EB_B64(1, 256, 2, 1)
-    EB_B64(2, 256, 1, 1)
-    EB_B64(3, 128, 4, 1)
+    EB_B64(0, 256, 2, 1)
+    EB_B64(1, 128, 4, 1)
+    EB_B64(2, 256, 2, 3)
+    EB_B64(3, 128, 4, 3)
     default: throw Error(EROSION_BAD_INPUT, "unknown FP64 batch shape");
   }
 #undef EB_B64
@@ -235,17 +235,20 @@ void launch_batch32(Batch& B, int shape, int njobs, long long items, cudaStream_
   EB_LAUNCH_CHECK();
 }
 
-static_assert(kFar64Shapes[1].nt == 256 && kFar64Shapes[1].tpt == 2 && kFar64Shapes[1].rcp == 1 &&
+static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Shapes[0].rcp == 1 &&
+              kFar64Shapes[1].nt == 128 && kFar64Shapes[1].tpt == 4 && kFar64Shapes[1].rcp == 1 &&
+              kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 2 && kFar64Shapes[2].rcp == 3 &&
+              kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 3 &&
               kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].rcp == 4,
               "launch_batch shape tables");
 
 // Chooses the ensemble launch shapes by timing each candidate on the jobs of
 // an all-FP64 and an all-FP32 round (zeroed strengths: same work).
 void occupancy(Batch& B) {
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[0], k_far64_batch<256, 2, 0>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[1], k_far64_batch<256, 2, 1>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[2], k_far64_batch<256, 1, 1>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[3], k_far64_batch<128, 4, 1>, 128, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[0], k_far64_batch<256, 2, 1>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[1], k_far64_batch<128, 4, 1>, 128, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[2], k_far64_batch<256, 2, 3>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[3], k_far64_batch<128, 4, 3>, 128, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[0], k_far32_batch<256, 4, 2>, 256, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[1], k_far32_batch<256, 4, 4>, 256, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[2], k_far32_batch<128, 4, 4>, 128, 0));
@@ -254,7 +257,7 @@ void occupancy(Batch& B) {
 
 void tune_batch(Batch& B, double pairs_total) {
   occupancy(B);
-  B.shape64 = 1;
+  B.shape64 = 0;
   B.shape32 = 0;
   for (int k = 0; k < 8; ++k) B.stats.tune_ms[k] = 0.f;
   if (pairs_total < kBatchTuneMinPairs) return;
@@ -268,7 +271,7 @@ void tune_batch(Batch& B, double pairs_total) {
     const std::vector<int> key(B.m.size(), kind);
     float best = 1e30f;
     const int nsh = kind ? kNumFar32Shapes : kNumFar64Shapes;
-    int bestsh = kind ? 0 : 1;
+    int bestsh = 0;
     for (int sh = 0; sh < nsh; ++sh) {
       if (kind) B.shape32 = sh;
       else B.shape64 = sh;
@@ -614,8 +617,9 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       s.st = mb.side;
       // the ensemble's far field runs in the ensemble's own launch shapes
       // (tune_batch), so the members skip the per-geometry timing
-      s.force_shape[0] = 1;
+      s.force_shape[0] = 0;
       s.force_shape[1] = 0;
+      s.force_shape[2] = 0;
       Problem pr;
       pr.P = P;
       if (npts[g] < 0 || nbods[g] < 0 || nouter[g] < 0) throw Error(EROSION_BAD_INPUT, "negative sizes");

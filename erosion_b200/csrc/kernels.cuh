@@ -230,6 +230,51 @@ __device__ __forceinline__ double rcp_newton(double r2) {
   return r2 > 0.0 ? y : 0.0;
 }
 
+// The FP64 hardware reciprocal estimate (rcp.approx.ftz.f64, a coarse
+// approximation formed from the upper half of the operand) refined by
+// Newton-Raphson steps y <- y + y (1 - r2 y) in FP64.  Each step squares the
+// relative error; NSTEP = 2 takes the estimate below FP64 rounding, NSTEP = 1
+// leaves a relative error of the order of the square of the estimate's.
+// r2 > 0 in the double's normal range (0 for r2 = 0, as rcp_or_zero).
+template <int NSTEP>
+__device__ __forceinline__ double rcp_newton64(double r2) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r2));
+#pragma unroll
+  for (int k = 0; k < NSTEP; ++k) {
+    const double e = fma(-r2, y, 1.0);
+    y = fma(y, e, y);
+  }
+  return r2 > 0.0 ? y : 0.0;
+}
+
+// One Newton-Raphson step from the FP32 estimate: relative error ~2^-46
+// (the estimate's ~2^-23, squared).  Same clamp and range as rcp_newton.
+__device__ __forceinline__ double rcp_newton1(double r2) {
+  float yf;
+  const float r2f = fminf(fmaxf(__double2float_rn(r2), 1.17549435e-38f), 3.40282347e38f);
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(r2f));
+  double y = (double)yf;
+  const double e = fma(-r2, y, 1.0);
+  y = fma(y, e, y);
+  return r2 > 0.0 ? y : 0.0;
+}
+
+// 1/r2 by variant: 0 correctly rounded division, 1 FP32 estimate + 2 Newton
+// steps, 3 FP64 estimate + 2 Newton steps (both at FP64 rounding: the
+// accurate FP64 operator); 2 FP32 estimate + 1 step, 4 FP64 estimate + 1 step
+// (relative error ~1e-14 and ~1e-12 per pair: the fast FP64 operator that the
+// mixed-precision solve applies while its residual is still large, where an
+// operator error far above FP64 rounding is harmless).
+template <int RCP>
+__device__ __forceinline__ double rcp_variant(double r2) {
+  if constexpr (RCP == 0) return rcp_or_zero(r2);
+  else if constexpr (RCP == 1) return rcp_newton(r2);
+  else if constexpr (RCP == 2) return rcp_newton1(r2);
+  else if constexpr (RCP == 3) return rcp_newton64<2>(r2);
+  else return rcp_newton64<1>(r2);
+}
+
 // One CTA's share of the FP64 far field: targets of block bx, tiles of split
 // 'split'.  Shared by k_far64 and the ensemble kernel k_far64_batch.
 template <bool MASK, int NT, int TPT, int RCP>
@@ -273,7 +318,7 @@ __device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __rest
         double rho2 = fma(rx, rx, ry * ry);
         double rdn = fma(rx, s.z, ry * s.w);
         double rds = fma(rx, a.x, ry * a.y);
-        double inv = RCP ? rcp_newton(rho2) : rcp_or_zero(rho2);
+        double inv = rcp_variant<RCP>(rho2);
         double c = rdn * rds * inv * inv;
         tx[q] = fma(c, rx, tx[q]);
         ty[q] = fma(c, ry, ty[q]);
@@ -551,13 +596,21 @@ k_far32_batch(const FarJob32* __restrict__ jobs, int njobs, long long nitems) {
 
 // Launch shapes the autotuner chooses from (threads per CTA, targets per
 // thread); solver.cu times each on the geometry at hand.
-// The third field is a kernel variant: for the FP64 kernel the reciprocal
-// (0 the division __drcp_rn, 1 rcp_newton), for the FP32 kernel the unroll
-// factor of the source loop.
+// The third field is a kernel variant: for the FP64 kernels the reciprocal
+// (rcp_variant), for the FP32 kernel the unroll factor of the source loop.
+// Kinds: 0 accurate FP64 (reciprocal at FP64 rounding), 1 FP32, 2 fast FP64.
 struct FarShape { int nt, tpt, rcp; };
-constexpr FarShape kFar64Shapes[] = {{256, 2, 0}, {256, 2, 1}, {256, 1, 1}, {128, 4, 1}};
+constexpr FarShape kFar64Shapes[] = {{256, 2, 1}, {128, 4, 1}, {256, 2, 3}, {128, 4, 3}};
 constexpr FarShape kFar32Shapes[] = {{256, 4, 2}, {256, 4, 4}, {128, 4, 4}, {128, 4, 2}};
-constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4;
+constexpr FarShape kFar64FastShapes[] = {{256, 2, 2}, {128, 4, 2}, {256, 2, 4}, {128, 4, 4}};
+constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4, kNumFar64FastShapes = 4;
+constexpr int kFarKinds = 3;
+constexpr FarShape far_shape_of(int kind, int i) {
+  return kind == 0 ? kFar64Shapes[i] : (kind == 1 ? kFar32Shapes[i] : kFar64FastShapes[i]);
+}
+constexpr int far_num_shapes(int kind) {
+  return kind == 0 ? kNumFar64Shapes : (kind == 1 ? kNumFar32Shapes : kNumFar64FastShapes);
+}
 
 // Tile centres (middle node) and, per node, the FP32 offset from its tile's
 // centre plus that centre (the target anchor of k_far32).  One CTA per tile.

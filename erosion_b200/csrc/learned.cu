@@ -1,16 +1,25 @@
 // Learned GMRES initial guess.  A small network maps per-body geometry
-// features to the body's density (its Fourier modes -8..8 and the stokeslet
-// and rotlet strengths); it is trained on densities the solver produced and
-// supplies the initial guess of the next solves.  Everything (features,
-// forward, backward, Adam, decoding) runs in the kernels of this file.
+// features, with the body's density increment over the previous time step,
+// to its increment over the current one; the guess is the previous step's
+// density plus the predicted increment.  It is trained on densities the
+// solver produced and supplies the initial guess of the next solves (GMRES
+// still iterates to the same tolerance, and the guess is used only when its
+// residual beats the previous step's density).  Everything (features,
+// forward, backward, Adam, encoding, decoding) runs in the kernels of this
+// file.
 //
-// Features of body b (LW_IN = 64), with R_b the mean radius (mean speed):
-//   28  Fourier modes +-2..+-8 of (z - c_b)/R_b on the offset grid (re, im)
+// Geometry features of body b (LW_GEO = 68), with R_b the mean radius (mean
+// speed):
+//   32  Fourier modes +-2..+-9 of (z - c_b)/R_b on the offset grid (re, im)
 //    4  log R_b, c_y/b, (b - |c_y| - R_b)/R_b, (a - |c_x| - R_b)/R_b
 //   32  the 8 nearest bodies: (dx, dy)/R_b, log(R_j/R_b), gap/R_b (clipped)
-// Targets (LW_OUT = 37): R_b * (modes -8..8 of sigma_x + i sigma_y), (re, im),
-//   then lambda_1, lambda_2, xi/R_b^2.
-// Network: 64 -> 256 -> 256 -> 256 -> 37, GELU on the hidden layers, weights
+// Density encoding (LW_OUT = 37): R_b * (modes -8..8 of sigma_x + i sigma_y),
+//   (re, im), then lambda_1, lambda_2, xi/R_b^2.  It is linear, so the
+//   encoding of an increment is the increment of the encodings.
+// Network input (LW_IN = 105): the geometry features, then the encoding of
+// the previous step's increment (zero when there is none); output: the
+// encoding of the current increment.
+// Network: 105 -> 256 -> 256 -> 256 -> 37, GELU on the hidden layers, weights
 // stored in BF16 for the forward and backward products (FP32 master copy for
 // Adam), FP32 accumulation.  Inputs and targets are standardised with the
 // training set's mean and deviation, which are part of the model.
@@ -23,7 +32,8 @@
 
 namespace {
 
-constexpr int LW_IN = 64, LW_H = 256, LW_OUT = 37, LW_K = 8, LW_NN = 8;
+constexpr int LW_GEO = 68, LW_H = 256, LW_OUT = 37, LW_K = 8, LW_KF = 9, LW_NN = 8;
+constexpr int LW_IN = LW_GEO + LW_OUT;
 constexpr int LW_LAYERS = 4;
 __host__ __device__ constexpr int lw_in(int l) { return l == 0 ? LW_IN : LW_H; }
 __host__ __device__ constexpr int lw_out(int l) { return l == LW_LAYERS - 1 ? LW_OUT : LW_H; }
@@ -35,17 +45,18 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return cdf + z * pdf;
 }
 
-// Per-body features, one CTA (128 threads) per body.
+// Per-body geometry features into row b of feat (row stride ld), one CTA
+// (128 threads) per body.
 __global__ void __launch_bounds__(128)
-k_lw_features(GeoDev G, double wall_a, double wall_b, float* __restrict__ feat) {
-  __shared__ double re[2 * LW_K + 1], im[2 * LW_K + 1];
+k_lw_features(GeoDev G, double wall_a, double wall_b, float* __restrict__ feat, int ld) {
+  __shared__ double re[2 * LW_KF + 1], im[2 * LW_KF + 1];
   const int b = blockIdx.x, n = G.n;
   const double2 c = G.cen[b];
   const double R = G.rb[b];
-  float* f = feat + (size_t)b * LW_IN;
-  // Fourier modes m = -K..K of (z - c)/R: one warp per mode, strided
-  for (int mi = threadIdx.x >> 5; mi < 2 * LW_K + 1; mi += blockDim.x >> 5) {
-    const int m = mi - LW_K;
+  float* f = feat + (size_t)b * ld;
+  // Fourier modes m = -KF..KF of (z - c)/R: one warp per mode, strided
+  for (int mi = threadIdx.x >> 5; mi < 2 * LW_KF + 1; mi += blockDim.x >> 5) {
+    const int m = mi - LW_KF;
     double sr = 0, si = 0;
     for (int k = threadIdx.x & 31; k < n; k += 32) {
       const double2 z = G.xy[G.nout + b * n + k];
@@ -63,10 +74,10 @@ k_lw_features(GeoDev G, double wall_a, double wall_b, float* __restrict__ feat) 
   __syncthreads();
   if (threadIdx.x == 0) {
     int q = 0;
-    for (int m = -LW_K; m <= LW_K; ++m) {
+    for (int m = -LW_KF; m <= LW_KF; ++m) {
       if (m >= -1 && m <= 1) continue;
-      f[q++] = (float)re[m + LW_K];
-      f[q++] = (float)im[m + LW_K];
+      f[q++] = (float)re[m + LW_KF];
+      f[q++] = (float)im[m + LW_KF];
     }
     f[q++] = (float)log(R);
     f[q++] = (float)(c.y / wall_b);
@@ -137,9 +148,10 @@ k_lw_encode(GeoDev G, const double* __restrict__ den, float* __restrict__ targ) 
   }
 }
 
-// Density from targets (decode) into the unknown vector; wall entries untouched.
+// Density from targets (decode) into the unknown vector, or added to it
+// (add = 1); wall entries untouched.
 __global__ void __launch_bounds__(128)
-k_lw_decode(GeoDev G, const float* __restrict__ targ, double* __restrict__ den) {
+k_lw_decode(GeoDev G, const float* __restrict__ targ, double* __restrict__ den, int add) {
   const int b = blockIdx.x, n = G.n;
   const double R = G.rb[b];
   const float* t = targ + (size_t)b * LW_OUT;
@@ -155,14 +167,24 @@ k_lw_decode(GeoDev G, const float* __restrict__ targ, double* __restrict__ den) 
       sy += ar * sn + ai * cs;
     }
     const int g = G.nout + b * n + k;
-    den[ix_of(G, g)] = sx;
-    den[iy_of(G, g)] = sy;
+    den[ix_of(G, g)] = add ? den[ix_of(G, g)] + sx : sx;
+    den[iy_of(G, g)] = add ? den[iy_of(G, g)] + sy : sy;
   }
   if (threadIdx.x == 0) {
-    den[ic_of(G, b, 0)] = t[34];
-    den[ic_of(G, b, 1)] = t[35];
-    den[ic_of(G, b, 2)] = (double)t[36] * R * R;
+    const double l1 = t[34], l2 = t[35], xi = (double)t[36] * R * R;
+    den[ic_of(G, b, 0)] = add ? den[ic_of(G, b, 0)] + l1 : l1;
+    den[ic_of(G, b, 1)] = add ? den[ic_of(G, b, 1)] + l2 : l2;
+    den[ic_of(G, b, 2)] = add ? den[ic_of(G, b, 2)] + xi : xi;
   }
+}
+
+// Row b of the network input: column LW_GEO.. of x gets the history hist[b]
+// (or zeros).
+__global__ void k_lw_put_hist(int M, const float* __restrict__ hist, float* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M * LW_OUT) return;
+  const int b = i / LW_OUT, c = i - b * LW_OUT;
+  x[(size_t)b * LW_IN + LW_GEO + c] = hist ? hist[i] : 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -359,7 +381,7 @@ static void lw_forward(State& s, LW& m, int B) {
   m.act.ensure((size_t)B * (LW_IN + 3 * LW_H + LW_OUT));
   m.pre.ensure((size_t)B * (3 * LW_H + LW_OUT));
   long long poff = 0;
-  // act layout: [x (B*64)] [h1] [h2] [h3] [y]
+  // act layout: [x (B*LW_IN)] [h1] [h2] [h3] [y]
   EB_CK(cudaMemcpyAsync(m.act.p, X, (size_t)B * LW_IN * sizeof(float), cudaMemcpyDeviceToDevice, s.st));
   aoff = (long long)B * LW_IN;
   const float* in = m.act.p;
@@ -432,15 +454,19 @@ static void lw_standardise(State& s, LW& m, const float* hx, const float* hy, lo
   EB_CK(cudaStreamSynchronize(s.st));
 }
 
-// Predicts targets (denormalised) for M bodies of the current geometry into d_out.
-void lw_predict_current(State& s, float* d_out, bool* ok) {
+// Predicts the encoded density increment (denormalised) of the M bodies of
+// the current geometry into d_out, given the previous increment's encoding
+// d_hist (M x LW_OUT, or null: none).
+void lw_predict_current(State& s, const float* d_hist, float* d_out, bool* ok) {
   LW& m = lw();
   *ok = m.ready && s.pr.M > 0;
   if (!*ok) return;
   const int M = s.pr.M;
   const GeoDev G = s.geo();
   m.xbuf.ensure((size_t)M * LW_IN);
-  k_lw_features<<<M, 128, 0, s.st>>>(G, s.pr.P.wall_a, s.pr.P.wall_b, m.xbuf.p);
+  k_lw_features<<<M, 128, 0, s.st>>>(G, s.pr.P.wall_a, s.pr.P.wall_b, m.xbuf.p, LW_IN);
+  EB_LAUNCH_CHECK();
+  k_lw_put_hist<<<nblk((long long)M * LW_OUT, 256), 256, 0, s.st>>>(M, d_hist, m.xbuf.p);
   EB_LAUNCH_CHECK();
   k_lw_scale<<<nblk((long long)M * LW_IN, 256), 256, 0, s.st>>>((long long)M * LW_IN, LW_IN, m.xbuf.p, m.d_xmean.p,
                                                                m.d_xsd.p, 0);
@@ -452,17 +478,27 @@ void lw_predict_current(State& s, float* d_out, bool* ok) {
   EB_LAUNCH_CHECK();
 }
 
-// Writes the learned density of every body into d_den (wall entries untouched).
-bool lw_guess_current(State& s, double* d_den) {
+// Adds the learned density increment of every body to d_den (which holds
+// the previous step's density; wall entries untouched).
+bool lw_guess_increment(State& s, const float* d_hist, double* d_den) {
   static DBuf<float> out;
   bool ok = false;
   out.ensure((size_t)std::max(1, s.pr.M) * LW_OUT);
-  lw_predict_current(s, out.p, &ok);
+  lw_predict_current(s, d_hist, out.p, &ok);
   if (!ok) return false;
-  k_lw_decode<<<s.pr.M, 128, 0, s.st>>>(s.geo(), out.p, d_den);
+  k_lw_decode<<<s.pr.M, 128, 0, s.st>>>(s.geo(), out.p, d_den, 1);
   EB_LAUNCH_CHECK();
   return true;
 }
+
+// The encoding (LW_OUT per body) of density d on the current geometry.
+void lw_encode_current(State& s, const double* d_den, float* d_out) {
+  if (s.pr.M == 0) return;
+  k_lw_encode<<<s.pr.M, 128, 0, s.st>>>(s.geo(), d_den, d_out);
+  EB_LAUNCH_CHECK();
+}
+
+int lw_out_width() { return LW_OUT; }
 
 }  // namespace eb
 
@@ -509,10 +545,10 @@ int erosion_lw_features(const erosion_params* p, int64_t npts, int64_t nbods, in
   return guarded4([&](State& s) {
     host_geometry(s, p, npts, nbods, nouter, xx, yy);
     static DBuf<float> f;
-    f.ensure((size_t)nbods * LW_IN);
-    k_lw_features<<<(unsigned)nbods, 128, 0, s.st>>>(s.geo(), s.pr.P.wall_a, s.pr.P.wall_b, f.p);
+    f.ensure((size_t)nbods * LW_GEO);
+    k_lw_features<<<(unsigned)nbods, 128, 0, s.st>>>(s.geo(), s.pr.P.wall_a, s.pr.P.wall_b, f.p, LW_GEO);
     EB_LAUNCH_CHECK();
-    d2h(feat, f.p, (size_t)nbods * LW_IN, s.st);
+    d2h(feat, f.p, (size_t)nbods * LW_GEO, s.st);
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
   });
@@ -542,12 +578,19 @@ int erosion_lw_decode(const erosion_params* p, int64_t npts, int64_t nbods, int6
     EB_CK(cudaMemsetAsync(dd, 0, s.pr.ntot * sizeof(double), s.st));
     static DBuf<float> t;
     h2d(t.ensure((size_t)nbods * LW_OUT), targ, (size_t)nbods * LW_OUT, s.st);
-    k_lw_decode<<<(unsigned)nbods, 128, 0, s.st>>>(s.geo(), t.p, dd);
+    k_lw_decode<<<(unsigned)nbods, 128, 0, s.st>>>(s.geo(), t.p, dd, 0);
     EB_LAUNCH_CHECK();
     d2h(density, dd, s.pr.ntot, s.st);
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
   });
+}
+
+int erosion_lw_dims(int32_t* geo, int32_t* in, int32_t* out) {
+  if (geo) *geo = LW_GEO;
+  if (in) *in = LW_IN;
+  if (out) *out = LW_OUT;
+  return EROSION_OK;
 }
 
 int erosion_lw_init(uint64_t seed) {

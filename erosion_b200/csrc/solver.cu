@@ -250,23 +250,29 @@ static void build_tiles(State& s) {
 // Far-field launch shapes and their autotuner.
 
 static int shape_targets(int kind, int shape) {
-  const FarShape sh = kind ? kFar32Shapes[shape] : kFar64Shapes[shape];
+  const FarShape sh = far_shape_of(kind, shape);
   return sh.nt * sh.tpt;
 }
 
-static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Shapes[0].rcp == 0 &&
-              kFar64Shapes[1].nt == 256 && kFar64Shapes[1].tpt == 2 && kFar64Shapes[1].rcp == 1 &&
-              kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 1 && kFar64Shapes[2].rcp == 1 &&
-              kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 1,
+static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Shapes[0].rcp == 1 &&
+              kFar64Shapes[1].nt == 128 && kFar64Shapes[1].tpt == 4 && kFar64Shapes[1].rcp == 1 &&
+              kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 2 && kFar64Shapes[2].rcp == 3 &&
+              kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 3,
               "launch_far's FP64 cases");
+static_assert(kFar64FastShapes[0].nt == 256 && kFar64FastShapes[0].tpt == 2 && kFar64FastShapes[0].rcp == 2 &&
+              kFar64FastShapes[1].nt == 128 && kFar64FastShapes[1].tpt == 4 && kFar64FastShapes[1].rcp == 2 &&
+              kFar64FastShapes[2].nt == 256 && kFar64FastShapes[2].tpt == 2 && kFar64FastShapes[2].rcp == 4 &&
+              kFar64FastShapes[3].nt == 128 && kFar64FastShapes[3].tpt == 4 && kFar64FastShapes[3].rcp == 4,
+              "launch_far's fast FP64 cases");
 static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[0].rcp == 2 &&
               kFar32Shapes[1].nt == 256 && kFar32Shapes[1].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
               kFar32Shapes[2].nt == 128 && kFar32Shapes[2].tpt == 4 && kFar32Shapes[2].rcp == 4 &&
               kFar32Shapes[3].nt == 128 && kFar32Shapes[3].tpt == 4 && kFar32Shapes[3].rcp == 2,
               "launch_far's FP32 cases");
 
-// One far-field launch of the given kind (0 FP64 on wrest, 1 FP32 on ws32)
-// and shape over the tile splits sp[0..nsplit], into out[split * N + i].
+// One far-field launch of the given kind (0 accurate FP64 and 2 fast FP64 on
+// wrest, 1 FP32 on ws32) and shape over the tile splits sp[0..nsplit], into
+// out[split * N + i].
 static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit, double2* out) {
   const Problem& pr = s.pr;
   const Near& nr = s.near;
@@ -298,13 +304,21 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
       EB_FAR32(3, 128, 4, 2)
       default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
     }
+  } else if (kind == 0) {
+    switch (shape) {
+      EB_FAR64(0, 256, 2, 1)
+      EB_FAR64(1, 128, 4, 1)
+      EB_FAR64(2, 256, 2, 3)
+      EB_FAR64(3, 128, 4, 3)
+      default: throw Error(EROSION_BAD_INPUT, "unknown FP64 far-field shape");
+    }
   } else {
     switch (shape) {
-      EB_FAR64(0, 256, 2, 0)
-      EB_FAR64(1, 256, 2, 1)
-      EB_FAR64(2, 256, 1, 1)
-      EB_FAR64(3, 128, 4, 1)
-      default: throw Error(EROSION_BAD_INPUT, "unknown FP64 far-field shape");
+      EB_FAR64(0, 256, 2, 2)
+      EB_FAR64(1, 128, 4, 2)
+      EB_FAR64(2, 256, 2, 4)
+      EB_FAR64(3, 128, 4, 4)
+      default: throw Error(EROSION_BAD_INPUT, "unknown fast FP64 far-field shape");
     }
   }
 #undef EB_FAR32
@@ -321,28 +335,33 @@ constexpr double kTuneMinPairs = 2e8;
 // (one warm-up and two timed launches on zeroed strengths, CUDA events on the
 // library stream) and the fastest kept.  The choice is cached per problem size
 // (N, tile count, masking), so an erosion run tunes once until a body is
-// deleted.
+// deleted.  Kinds 0 and 2 (accurate and fast FP64) sum every tile; kind 1
+// (FP32) the body tiles, and the mixed operator adds the wall tiles in the
+// kind-0 shape.
 static void plan_far(State& s) {
   const Problem& pr = s.pr;
   // the FP32 kernel sums the body tiles; the wall's tiles (first nwall_tiles)
   // always run in FP64 (their densities carry fields that cancel against the
   // bodies' to a few parts in 1e4, beyond FP32's reach)
   const int t32 = s.nwall_tiles, n32 = s.ntile - s.nwall_tiles;
-  int max64 = s.nsplit, max32 = 0, maxw = 0;
-  for (int sh = 0; sh < kNumFar64Shapes; ++sh) {
-    max64 = std::max(max64, far_split_count(pr.N, s.ntile, shape_targets(0, sh)));
-    maxw = std::max(maxw, far_split_count(pr.N, s.nwall_tiles, shape_targets(0, sh)));
-  }
-  for (int sh = 0; sh < kNumFar32Shapes && n32 > 0; ++sh)
-    max32 = std::max(max32, far_split_count(pr.N, n32, shape_targets(1, sh)));
-  s.partial.ensure((size_t)std::max(max64, max32 + maxw) * pr.N);
+  int maxs = s.nsplit, max32 = 0, maxw = 0;
+  for (int kind = 0; kind < kFarKinds; ++kind)
+    for (int sh = 0; sh < far_num_shapes(kind); ++sh) {
+      if (kind == 1) {
+        if (n32 > 0) max32 = std::max(max32, far_split_count(pr.N, n32, shape_targets(1, sh)));
+      } else {
+        maxs = std::max(maxs, far_split_count(pr.N, s.ntile, shape_targets(kind, sh)));
+        maxw = std::max(maxw, far_split_count(pr.N, s.nwall_tiles, shape_targets(kind, sh)));
+      }
+    }
+  s.partial.ensure((size_t)std::max(maxs, max32 + maxw) * pr.N);
   const int masked = s.near.npairs > 0;
   const bool tune = (double)pr.N * (double)pr.N >= kTuneMinPairs;
   const bool cached = s.tune_N == pr.N && s.tune_ntile == s.ntile && s.tune_masked == masked;
   bool zeroed = false;
-  for (int kind = 0; kind < 2; ++kind) {
-    const int nsh = kind ? kNumFar32Shapes : kNumFar64Shapes;
-    const int tb = kind ? t32 : 0, tcount = kind ? n32 : s.ntile;
+  for (int kind = 0; kind < kFarKinds; ++kind) {
+    const int nsh = far_num_shapes(kind);
+    const int tb = kind == 1 ? t32 : 0, tcount = kind == 1 ? n32 : s.ntile;
     if (tcount == 0) { s.nsplit32 = 0; s.far_shape[kind] = 0; continue; }
     int best = 0;
     if (s.force_shape[kind] >= 0) {
@@ -378,7 +397,8 @@ static void plan_far(State& s) {
     s.far_shape[kind] = best;
     const int ns = far_split_count(pr.N, tcount, shape_targets(kind, best));
     if (kind == 1) { s.nsplit32 = ns; upload_splits(s, s.split_ptr32, ns, tb, tb + tcount); }
-    else { s.nsplit64t = ns; upload_splits(s, s.split_ptr64t, ns, 0, s.ntile); }
+    else if (kind == 0) { s.nsplit64t = ns; upload_splits(s, s.split_ptr64t, ns, 0, s.ntile); }
+    else { s.nsplit64f = ns; upload_splits(s, s.split_ptr64f, ns, 0, s.ntile); }
   }
   // the wall-source FP64 launch of the mixed operator, in the FP64 shape
   s.nsplitw = far_split_count(pr.N, s.nwall_tiles, shape_targets(0, s.far_shape[0]));
@@ -474,7 +494,7 @@ void record_setup_stats(State& s) {
   s.stats.ms_precond_setup = s.pc_setup_ms;
 }
 
-bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned) {
+bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned, const float* d_hist) {
   for (int q = 0; q < 3; ++q) s.stats.guess_residual[q] = -1.0;
   s.stats.guess_residual[0] = 1.0;
   const long long N = s.pr.ntot;
@@ -502,10 +522,9 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
   static DBuf<double> cand;
   double* c = cand.ensure(N);
   if (have_x) EB_CK(cudaMemcpyAsync(c, d_x, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  else EB_CK(cudaMemsetAsync(c, 0, N * sizeof(double), st));
-  if (lw_guess_current(s, c)) {
-    // the network predicts the bodies only: complete the wall density with
-    // Richardson sweeps on the wall rows (wall block ~ -1/2 I)
+  if (have_x && lw_guess_increment(s, d_hist, c)) {
+    // the network predicts the bodies' increment only: update the wall
+    // density by Richardson sweeps on the wall rows (wall block ~ -1/2 I)
     for (int it = 0; it < 3; ++it) {
       rel_res(c);
       k_wall_richardson<<<nblk(2LL * s.pr.nout, 256), 256, 0, st>>>(s.pr.nout, r, c);
@@ -527,11 +546,23 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
 
 void setup_preconditioner(State& s) {
   const Problem& pr = s.pr;
+  s.pc_setup_ms = 0.0;
+  if (pr.P.precond != 1 || pr.M == 0) {
+    s.pc_active = false;
+    s.pc_singular = 0;
+    return;
+  }
+  const int n = pr.n, m = 2 * n + 3;
+  // keep the previous inverses (a lagged preconditioner) when allowed
+  if (pr.P.precond_refresh > 1 && s.pc_valid && s.pc_M == pr.M && s.pc_n == n && s.pc_nout == pr.nout &&
+      s.pc_age + 1 < pr.P.precond_refresh) {
+    s.pc_age++;
+    s.pc_active = s.pc_singular < pr.M;
+    return;
+  }
   s.pc_active = false;
   s.pc_singular = 0;
-  s.pc_setup_ms = 0.0;
-  if (pr.P.precond != 1 || pr.M == 0) return;
-  const int n = pr.n, m = 2 * n + 3;
+  s.pc_valid = false;
   const GeoDev G = s.geo();
   EB_CK(cudaEventRecord(s.et0, s.st));
   float* B = s.pcB.ensure((size_t)pr.M * m * m);
@@ -566,6 +597,11 @@ void setup_preconditioner(State& s) {
   s.pc_tw.ensure((size_t)s.pc_wsplit * pr.M * n);
   s.pc_ws32.ensure(pr.nout);
   s.pc_active = s.pc_singular < pr.M;
+  s.pc_valid = true;
+  s.pc_M = pr.M;
+  s.pc_n = n;
+  s.pc_nout = pr.nout;
+  s.pc_age = 0;
 }
 
 void apply_preconditioner(State& s, const double* v, double* z) {
@@ -589,6 +625,7 @@ void harvest_far_timing(State& s) {
     EB_CK(cudaEventSynchronize(s.ef1));   // complete already on every path that calls this
     EB_CK(cudaEventElapsedTime(&ms, s.ef0, s.ef1));
     if (s.far_kind == 1) s.stats.ms_far32 += ms;
+    else if (s.far_kind == 2) s.stats.ms_far64f += ms;
     else s.stats.ms_far += ms;
     s.far_pending = false;
   }
@@ -607,7 +644,9 @@ void operator_prep(State& s, const double* d_den, double* d_vel) {
   EB_LAUNCH_CHECK();
 }
 
-int far_slots(const State& s, int prec) { return prec == 1 ? s.nsplit32 + s.nsplitw : s.nsplit64t; }
+int far_slots(const State& s, int prec) {
+  return prec == 1 ? s.nsplit32 + s.nsplitw : (prec == 2 ? s.nsplit64f : s.nsplit64t);
+}
 
 void operator_post(State& s, const double* d_den, double* d_vel, int nsplit) {
   const Problem& pr = s.pr;
@@ -635,11 +674,12 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
   const Problem& pr = s.pr;
   cudaStream_t st = s.st;
   operator_prep(s, d_den, d_vel);
-  const int kind = prec == 1 ? 1 : 0;
-  const int n1 = kind ? s.nsplit32 : s.nsplit64t;
+  const int kind = prec == 1 ? 1 : (prec == 2 ? 2 : 0);
+  const int n1 = kind == 1 ? s.nsplit32 : (kind == 2 ? s.nsplit64f : s.nsplit64t);
   if (n1 > 0) {
     EB_CK(cudaEventRecord(s.ef0, st));
-    launch_far(s, kind, s.far_shape[kind], kind ? s.split_ptr32.p : s.split_ptr64t.p, n1, s.partial.p);
+    launch_far(s, kind, s.far_shape[kind],
+               kind == 1 ? s.split_ptr32.p : (kind == 2 ? s.split_ptr64f.p : s.split_ptr64t.p), n1, s.partial.p);
     EB_CK(cudaEventRecord(s.ef1, st));
     s.far_kind = kind;
     s.far_pending = true;
@@ -653,6 +693,8 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
     s.stats.matvecs_fp32++;
     if (s.nsplit32 > 0) s.stats.far32_launches++;
     s.stats.farw_launches++;
+  } else if (kind == 2) {
+    s.stats.far64f_launches++;
   } else {
     s.stats.far_launches++;
   }
@@ -757,7 +799,9 @@ static int gmres_cycle(State& s, double* d_r, double* d_x, long long maxl_in, do
     }
     double* V = s.V.p;
     double* vnew = V + ll * ldv;
-    const int prec = (relax_abs > 0.0 && rho < relax_abs) ? 1 : 0;
+    // mixed precision: the fast FP64 operator while the residual is large,
+    // the FP32 far field once it is below relax_abs
+    const int prec = relax_abs > 0.0 ? (rho < relax_abs ? 1 : (s.pr.P.fast_fp64 ? 2 : 0)) : 0;
     if (s.pc_active) {
       // flexible GMRES: keep z_k = P^{-1} v_k so that x = x0 + Z y is exactly
       // consistent with the Arnoldi relation A Z = V H whatever the
@@ -937,9 +981,11 @@ void release_state_buffers(State& s) {
   s.vcap = 0;
   s.zcap = 0;
   s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
+  s.pc_valid = false;
   s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
   s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();
-  s.split_tune.release(); s.tune_N = -1; s.tuned_shape[0] = s.tuned_shape[1] = -1;
+  s.split_tune.release(); s.split_ptr64f.release(); s.tune_N = -1;
+  for (int k = 0; k < kFarKinds; ++k) s.tuned_shape[k] = -1;
   s.dker_body_n = s.dker_wall_n = -1;
   s.geo_valid = false;
 }
@@ -1045,6 +1091,7 @@ void erosion_default_params(erosion_params* p) {
   p->precision = 0;
   p->rhs_mode = 0;
   p->true_residual = 0;
+  p->fast_fp64 = 1;
 }
 
 int erosion_last_status(void) { return t_status; }
@@ -1116,7 +1163,9 @@ int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t
     double* dd = s.d_den.ensure(ntot);
     double* dv = s.d_w.ensure(ntot);
     h2d(dd, density, ntot, s.st);
-    apply_operator(s, dd, dv, s.pr.P.precision == 1 ? 1 : 0);
+    const int prec = s.pr.P.precision;
+    if (prec < 0 || prec > 2) throw Error(EROSION_BAD_INPUT, "precision must be 0, 1 or 2");
+    apply_operator(s, dd, dv, prec);
     d2h(vel, dv, ntot, s.st);
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
@@ -1191,24 +1240,24 @@ int64_t erosion_launch_count(void) { return (int64_t)g_launches; }
 int erosion_set_far_shape(int32_t kind, int32_t shape) {
   State& s = state();
   std::lock_guard<std::mutex> lk(s.mu);
-  const int nsh = kind == 0 ? kNumFar64Shapes : kNumFar32Shapes;
-  if ((kind != 0 && kind != 1) || shape < -1 || shape >= nsh) {
+  if (kind < 0 || kind >= kFarKinds || shape < -1 || shape >= far_num_shapes(kind)) {
     set_status(EROSION_BAD_INPUT, "unknown far-field kernel kind or shape");
     return EROSION_BAD_INPUT;
   }
   s.force_shape[kind] = shape;
+  set_status(EROSION_OK, "");
   return EROSION_OK;
 }
 
 int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* num_shapes) {
   State& s = state();
   std::lock_guard<std::mutex> lk(s.mu);
-  for (int kind = 0; kind < 2; ++kind) {
-    const int nsh = kind ? kNumFar32Shapes : kNumFar64Shapes;
+  for (int kind = 0; kind < kFarKinds; ++kind) {
+    const int nsh = far_num_shapes(kind);
     if (shape) shape[kind] = s.far_shape[kind];
     if (num_shapes) num_shapes[kind] = nsh;
     for (int i = 0; i < nsh; ++i) {
-      const FarShape sh = kind ? kFar32Shapes[i] : kFar64Shapes[i];
+      const FarShape sh = far_shape_of(kind, i);
       if (desc) {
         desc[12 * kind + 3 * i] = sh.nt;
         desc[12 * kind + 3 * i + 1] = sh.tpt;

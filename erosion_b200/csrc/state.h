@@ -123,16 +123,17 @@ struct State {
 
   // far field
   DBuf<int4> tiles;
-  DBuf<int> split_ptr, split_ptr32, split_ptr64t, split_ptrw, split_tune;
-  int nsplit = 0, nsplit32 = 0, nsplit64t = 0, nsplitw = 0, ntile = 0;
+  DBuf<int> split_ptr, split_ptr32, split_ptr64t, split_ptr64f, split_ptrw, split_tune;
+  int nsplit = 0, nsplit32 = 0, nsplit64t = 0, nsplit64f = 0, nsplitw = 0, ntile = 0;
   long long far64_pairs = 0, farw_pairs = 0;   // pairs per full FP64 / wall-source launch
   // far-field launch shapes: index into the candidate lists of kernels.cuh
   // (kind 0 FP64, 1 FP32), chosen by the autotuner or forced by the caller
-  int far_shape[2] = {0, 0};
-  int force_shape[2] = {-1, -1};
-  int tuned_shape[2] = {-1, -1};
+  // (kind 0 accurate FP64, 1 FP32, 2 fast FP64)
+  int far_shape[3] = {0, 0, 0};
+  int force_shape[3] = {-1, -1, -1};
+  int tuned_shape[3] = {-1, -1, -1};
   int tune_N = -1, tune_ntile = -1, tune_masked = -1;
-  float tune_ms[2][8] = {};
+  float tune_ms[3][8] = {};
   cudaEvent_t et0 = nullptr, et1 = nullptr;
   // mixed precision: FP32 geometry, strengths, self-curve tasks and sums
   DBuf<float4> src32;
@@ -152,9 +153,11 @@ struct State {
   DBuf<float2> pc_ws32;     // wall strengths of the coupling sum
   DBuf<int> pc_bad;         // per body: 1 when its block had a zero pivot
   int pc_singular = 0;      // bodies left unpreconditioned
+  bool pc_valid = false;    // pcB holds inverses of a (pc_M, pc_n) problem
+  int pc_M = -1, pc_n = -1, pc_nout = -1, pc_age = 0;   // ... built pc_age set-ups ago
   double pc_setup_ms = 0.0; // device time of block assembly + inversion
   double setup_ms = 0.0;    // host wall time of the last setup_problem
-  int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32
+  int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32, 2 fast FP64
 
   // work buffers
   DBuf<double2> ws, wrest, partial, bd, pair_out;
@@ -205,13 +208,22 @@ void build_rhs(State& s, double* d_rhs);
 // GMRES (SLATEC DGMRES semantics, CGS2 Arnoldi); returns EROSION_* status.
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
                 long long* iters, double* est);
-// Initial guess selection: candidates zero, the supplied d_x (have_x) and,
-// with learned, the network's guess; d_x receives the one with the smallest
-// FP64 residual.  Returns true when that is the zero vector.
-bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned);
-// Writes the learned density of every body into d_den (wall untouched);
-// false when no trained network exists.
-bool lw_guess_current(State& s, double* d_den);
+// Initial guess selection: candidates zero, the supplied d_x (have_x: the
+// previous step's density) and, with learned and have_x, that density plus
+// the network's predicted increment (d_hist: the encoded previous
+// increment, or null); d_x receives the one with the smallest FP64
+// residual.  Returns true when that is the zero vector.
+bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned,
+                          const float* d_hist = nullptr);
+// Adds the learned density increment of every body to d_den (the previous
+// step's density; wall untouched), given the encoding of the previous
+// increment d_hist (nbods x lw_out_width(), or null); false when no trained
+// network exists.
+bool lw_guess_increment(State& s, const float* d_hist, double* d_den);
+// The learned part's density encoding (lw_out_width() floats per body) of
+// d_den on the current geometry.
+void lw_encode_current(State& s, const double* d_den, float* d_out);
+int lw_out_width();
 // Builds (or disables) the block preconditioner for the current geometry.
 void setup_preconditioner(State& s);
 // Copies the last set-up's figures (time, preconditioner state) into s.stats.

@@ -161,12 +161,214 @@ k_stress_trap(GeoDev G, const double* __restrict__ den, const int4* __restrict__
   }
 }
 
+// ---- Shear stress with the trapezoid rule wherever it is exact to rounding.
+// The reference evaluates every other curve's contribution to a body node by
+// the barycentric formulas (deformation_on_boundary, :2707-2727 and
+// :2893-2925).  Away from a source curve the trapezoid rule on the same
+// density gives the same value up to its quadrature (aliasing) error, which
+// for a density with content up to the Nyquist mode decays like
+// exp(-pi d / h) with the distance d to the curve and its node spacing h:
+// beyond d = STRESS_NEAR_H h it is below 1e-16 of the value.  So the
+// barycentric evaluation runs only on the (body node, source curve) pairs
+// within that distance, and the trapezoid rule (FP64) on all the others.
+constexpr double STRESS_NEAR_H = 12.0;
+
+// Per body node: min over wall nodes j of |x_i - x_j|^2 / h_j^2, with h_j the
+// local wall spacing |z'_j| 2 pi / nout.  Wall nodes staged through shared
+// memory in chunks.
+__global__ void __launch_bounds__(256)
+k_stress_wall_dist(GeoDev G, double* __restrict__ d2h) {
+  __shared__ double2 sxy[256];
+  __shared__ double sh2[256];
+  const int nb = G.n * G.M;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double2 p = G.xy[G.nout + (i < nb ? i : nb - 1)];
+  const double hs = EB_TWOPI / G.nout;
+  double best = 1e300;
+  for (int j0 = 0; j0 < G.nout; j0 += 256) {
+    __syncthreads();
+    const int j = j0 + threadIdx.x;
+    if (j < G.nout) {
+      sxy[threadIdx.x] = G.xy[j];
+      const double h = G.sp[j] * hs;
+      sh2[threadIdx.x] = 1.0 / (h * h);
+    }
+    __syncthreads();
+    const int jt = min(256, G.nout - j0);
+    for (int k = 0; k < jt; ++k) {
+      const double dx = p.x - sxy[k].x, dy = p.y - sxy[k].y;
+      best = fmin(best, (dx * dx + dy * dy) * sh2[k]);
+    }
+  }
+  if (i < nb) d2h[i] = best;
+}
+
+// Per body: radius of the smallest centroid-centred disc holding its nodes,
+// and its node spacing (mean speed x 2 pi / n).
+__global__ void __launch_bounds__(256)
+k_body_extent(GeoDev G, double2* __restrict__ ext) {
+  __shared__ double red[32];
+  const int b = blockIdx.x;
+  const double2 c = G.cen[b];
+  double r = 0.0;
+  for (int k = threadIdx.x; k < G.n; k += blockDim.x) {
+    const double2 p = G.xy[G.nout + b * G.n + k];
+    r = fmax(r, sqrt((p.x - c.x) * (p.x - c.x) + (p.y - c.y) * (p.y - c.y)));
+  }
+  // block max: within each warp, then across the warps
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+    if (threadIdx.x == 0) ext[b] = make_double2(r, G.rb[b] * EB_TWOPI / G.n);
+  }
+}
+
+// Near mask of the stress: bit c of mask[i * mw + c/32] is set when body node
+// i lies within STRESS_NEAR_H node spacings of source curve c (its own body
+// excluded): for the wall from k_stress_wall_dist, for a body by its bounding
+// disc.
+__global__ void __launch_bounds__(256)
+k_stress_near_mask(GeoDev G, const double* __restrict__ wall_d2h, const double2* __restrict__ ext, int mw,
+                   unsigned* __restrict__ mask) {
+  const int nb = G.n * G.M;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const int own = 1 + i / G.n;
+  const double2 p = G.xy[G.nout + i];
+  for (int w = 0; w < mw; ++w) {
+    unsigned bits = 0u;
+    for (int q = 0; q < 32; ++q) {
+      const int c = 32 * w + q;
+      if (c > G.M) break;
+      bool near;
+      if (c == 0) {
+        near = wall_d2h[i] <= STRESS_NEAR_H * STRESS_NEAR_H;
+      } else if (c == own) {
+        near = false;
+      } else {
+        const double2 cc = G.cen[c - 1], e = ext[c - 1];
+        const double R = e.x + STRESS_NEAR_H * e.y;
+        const double dx = p.x - cc.x, dy = p.y - cc.y;
+        near = dx * dx + dy * dy <= R * R;
+      }
+      if (near) bits |= 1u << q;
+    }
+    mask[(size_t)i * mw + w] = bits;
+  }
+}
+
+// Barycentric Stokes DLP gradient of the near source curves only: CTA = task
+// (up to NEAR_NT nodes of one body); the CTA visits, in curve order, every
+// curve that is near for at least one of its nodes, and a node keeps the
+// value only for the curves near to it.  out[q * nb + i], q as k_bary_sum
+// (one split).
+__global__ void __launch_bounds__(NEAR_NT)
+k_bary_sum_near(GeoDev G, const double2* __restrict__ bd_all, const int4* __restrict__ tasks,
+                const unsigned* __restrict__ mask, int mw, double* __restrict__ out) {
+  __shared__ BaryTile T;
+  __shared__ unsigned tmask;
+  const int nb = G.n * G.M;
+  const int4 tk = tasks[blockIdx.x];
+  const int t = tk.x + threadIdx.x;
+  const bool act = t < tk.y;
+  const int tc = act ? t : tk.y - 1;
+  const double2 zt = G.xy[G.nout + tc];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int w = 0; w < mw; ++w) {
+    const unsigned my = act ? mask[(size_t)tc * mw + w] : 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) tmask = 0u;
+    __syncthreads();
+    const unsigned wor = __reduce_or_sync(0xffffffffu, my);
+    if ((threadIdx.x & 31) == 0 && wor) atomicOr(&tmask, wor);
+    __syncthreads();
+    unsigned bits = tmask;   // block-uniform
+    while (bits) {
+      const int q = __ffs(bits) - 1;
+      bits &= bits - 1u;
+      const int c = 32 * w + q;
+      DLPVal r = bary_eval<2>(T, G, c, bd_all + bd_all_off(G, c), zt, act);
+      if ((my >> q) & 1u) {
+        a[0] += r.ux; a[1] += r.uy; a[2] += r.u1x; a[3] += r.u1y; a[4] += r.u2x; a[5] += r.u2y;
+      }
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) out[(size_t)q * nb + t] = a[q];
+  }
+}
+
+// Trapezoid deformation tensor of every other curve except the near ones
+// (mask as k_stress_near_mask), as partial sums over the far-field tile
+// splits: out[(split*3 + q)*nb + i].  The same terms as k_stress_trap, the
+// density scaled by the weight when staged and the reciprocal by
+// rcp_newton.
+__global__ void __launch_bounds__(256)
+k_stress_far(GeoDev G, const double* __restrict__ den, const int4* __restrict__ tiles,
+             const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
+             double* __restrict__ out) {
+  __shared__ double4 sg[FAR_TS];   // x, y, nx, ny
+  __shared__ double2 ss[FAR_TS];   // w sigma
+  const int nb = G.n * G.M;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < nb;
+  const int ic = act ? i : nb - 1;
+  const int g = G.nout + ic;
+  const int mycurve = 1 + ic / G.n;
+  const double2 p = G.xy[g];
+  double e11 = 0, e12 = 0, e22 = 0;
+  const int split = blockIdx.y;
+  for (int ti = split_ptr[split]; ti < split_ptr[split + 1]; ++ti) {
+    const int4 T = tiles[ti];
+    __syncthreads();
+    for (int k = threadIdx.x; k < T.y; k += blockDim.x) {
+      const int gs = T.x + k;
+      const double2 q = G.xy[gs], nn = G.nrm[gs];
+      const double wg = G.w[gs];
+      sg[k] = make_double4(q.x, q.y, nn.x, nn.y);
+      ss[k] = make_double2(den[ix_of(G, gs)] * wg, den[iy_of(G, gs)] * wg);
+    }
+    __syncthreads();
+    if (T.z == mycurve || ((__ldg(mask + (size_t)ic * mw + (T.z >> 5)) >> (T.z & 31)) & 1u)) continue;
+    double a11 = 0, a12 = 0, a22 = 0;
+#pragma unroll 2
+    for (int j = 0; j < T.y; ++j) {
+      const double4 q = sg[j];
+      const double2 sd = ss[j];
+      const double rx = p.x - q.x, ry = p.y - q.y;
+      const double inv = rcp_newton(fma(rx, rx, ry * ry));
+      const double i4 = inv * inv;
+      const double rdn = fma(rx, q.z, ry * q.w), rtn = fma(rx, q.w, ry * q.z);
+      const double rds = fma(rx, sd.x, ry * sd.y), rts = fma(rx, sd.y, ry * sd.x);
+      const double A = rdn * rds * i4;
+      const double C = 4.0 * A * inv;
+      a11 += A + i4 * rx * fma(rds, q.z, rdn * sd.x) - C * rx * rx;
+      a22 += A + i4 * ry * fma(rds, q.w, rdn * sd.y) - C * ry * ry;
+      a12 += 0.5 * i4 * fma(rds, rtn, rdn * rts) - C * rx * ry;
+    }
+    e11 += a11; e12 += a12; e22 += a22;
+  }
+  if (act) {
+    out[((size_t)split * 3 + 0) * nb + i] = e11;
+    out[((size_t)split * 3 + 1) * nb + i] = e12;
+    out[((size_t)split * 3 + 2) * nb + i] = e22;
+  }
+}
+
 // Deformation tensor assembly, stokeslet/rotlet gradients (:2964-2994; the
 // trapezoid variant flips the sign of the rotlet's E22 term, :2604-2605),
 // traction -2 E n and shear stress tau = f.(p_y, -p_x) (:3075-3092).
+// part_b: barycentric partial sums (6 per split, NDER = 2 layout of
+// k_bary_sum), part_t: trapezoid partial sums (3 per split, k_stress_trap and
+// k_stress_far layout); either count may be zero.
 __global__ void __launch_bounds__(256)
-k_stress_final(GeoDev G, const double* __restrict__ den, const double* __restrict__ part, int nsplit, int bary,
-               const double* __restrict__ eself, double* __restrict__ tau, double* __restrict__ Eout) {
+k_stress_final(GeoDev G, const double* __restrict__ den, const double* __restrict__ part_b, int nsplit_b,
+               const double* __restrict__ part_t, int nsplit_t, int bary, const double* __restrict__ eself,
+               double* __restrict__ tau, double* __restrict__ Eout) {
   __shared__ double4 sc[SR_CHUNK];
   __shared__ double sr[SR_CHUNK];
   const int nb = G.n * G.M;
@@ -174,18 +376,17 @@ k_stress_final(GeoDev G, const double* __restrict__ den, const double* __restric
   const bool act = i < nb;
   const int ic = act ? i : nb - 1;
   double e11 = 0, e12 = 0, e22 = 0;
-  for (int s = 0; s < nsplit; ++s) {
-    if (bary) {
-      const double* P = part + (size_t)s * 6 * nb;
-      e11 += P[2 * (size_t)nb + ic];
-      e12 += 0.5 * (P[3 * (size_t)nb + ic] + P[4 * (size_t)nb + ic]);
-      e22 += P[5 * (size_t)nb + ic];
-    } else {
-      const double* P = part + (size_t)s * 3 * nb;
-      e11 += P[ic];
-      e12 += P[(size_t)nb + ic];
-      e22 += P[2 * (size_t)nb + ic];
-    }
+  for (int s = 0; s < nsplit_b; ++s) {
+    const double* P = part_b + (size_t)s * 6 * nb;
+    e11 += P[2 * (size_t)nb + ic];
+    e12 += 0.5 * (P[3 * (size_t)nb + ic] + P[4 * (size_t)nb + ic]);
+    e22 += P[5 * (size_t)nb + ic];
+  }
+  for (int s = 0; s < nsplit_t; ++s) {
+    const double* P = part_t + (size_t)s * 3 * nb;
+    e11 += P[ic];
+    e12 += P[(size_t)nb + ic];
+    e22 += P[2 * (size_t)nb + ic];
   }
   e11 += eself[ic];
   e12 += eself[nb + ic];
@@ -488,31 +689,61 @@ void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E) {
   k_stress_self<<<pr.M, 256, smem, s.st>>>(G, d_den, s.dker_body.p, eself.p);
   EB_LAUNCH_CHECK();
   const int bary = pr.P.ibary == 1;
-  int nsplit = 0;
-  if (bary) {
+  if (bary && pr.P.stress_all_bary) {   // every pair barycentric, as the reference evaluates it
     bdval_all(s, d_den, bd_all);
     std::vector<int4> tasks;
     for (int b = 0; b < pr.M; ++b)
       for (int k0 = 0; k0 < pr.n; k0 += NEAR_NT)
         tasks.push_back(make_int4(b * pr.n + k0, b * pr.n + std::min(pr.n, k0 + NEAR_NT), 1 + b, 0));
     std::vector<int> sc;
-    nsplit = source_splits((int)tasks.size(), pr.M + 1, sc);
+    const int nsplit = source_splits((int)tasks.size(), pr.M + 1, sc);
     h2d(d_tasks.ensure(tasks.size()), tasks.data(), tasks.size(), s.st);
     h2d(d_sc.ensure(sc.size()), sc.data(), sc.size(), s.st);
     part.ensure((size_t)nsplit * 6 * nb);
     dim3 grid((unsigned)tasks.size(), nsplit);
     k_bary_sum<2><<<grid, NEAR_NT, 0, s.st>>>(G, bd_all.p, d_tasks.p, s.xy.p + pr.nout, d_sc.p, nb, part.p);
     EB_LAUNCH_CHECK();
+    k_stress_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, part.p, nsplit, nullptr, 0, 1, eself.p, d_tau, d_E);
+    EB_LAUNCH_CHECK();
     EB_CK(cudaStreamSynchronize(s.st));
+  } else if (bary) {   // barycentric near pairs, trapezoid elsewhere
+    static DBuf<double> wall_d2h;
+    static DBuf<double2> ext;
+    static DBuf<unsigned> smask;
+    static DBuf<double> pnear;
+    const int mw = (pr.M + 1 + 31) / 32;
+    k_stress_wall_dist<<<nblk(nb, 256), 256, 0, s.st>>>(G, wall_d2h.ensure(nb));
+    EB_LAUNCH_CHECK();
+    k_body_extent<<<pr.M, 256, 0, s.st>>>(G, ext.ensure(pr.M));
+    EB_LAUNCH_CHECK();
+    k_stress_near_mask<<<nblk(nb, 256), 256, 0, s.st>>>(G, wall_d2h.p, ext.p, mw, smask.ensure((size_t)nb * mw));
+    EB_LAUNCH_CHECK();
+    bdval_all(s, d_den, bd_all);
+    std::vector<int4> tasks;
+    for (int b = 0; b < pr.M; ++b)
+      for (int k0 = 0; k0 < pr.n; k0 += NEAR_NT)
+        tasks.push_back(make_int4(b * pr.n + k0, b * pr.n + std::min(pr.n, k0 + NEAR_NT), 1 + b, 0));
+    h2d(d_tasks.ensure(tasks.size()), tasks.data(), tasks.size(), s.st);
+    k_bary_sum_near<<<(unsigned)tasks.size(), NEAR_NT, 0, s.st>>>(G, bd_all.p, d_tasks.p, smask.p, mw,
+                                                                   pnear.ensure(6LL * nb));
+    EB_LAUNCH_CHECK();
+    const int nsplit = s.nsplit;
+    part.ensure((size_t)nsplit * 3 * nb);
+    k_stress_far<<<dim3(nblk(nb, 256), nsplit), 256, 0, s.st>>>(G, d_den, s.tiles.p, s.split_ptr.p, smask.p, mw,
+                                                                 part.p);
+    EB_LAUNCH_CHECK();
+    k_stress_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, pnear.p, 1, part.p, nsplit, 1, eself.p, d_tau, d_E);
+    EB_LAUNCH_CHECK();
+    EB_CK(cudaStreamSynchronize(s.st));   // the task list goes out of scope
   } else {
-    nsplit = s.nsplit;
+    const int nsplit = s.nsplit;
     part.ensure((size_t)nsplit * 3 * nb);
     dim3 grid(nblk(nb, 256), nsplit);
     k_stress_trap<<<grid, 256, 0, s.st>>>(G, d_den, s.tiles.p, s.split_ptr.p, part.p);
     EB_LAUNCH_CHECK();
+    k_stress_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, nullptr, 0, part.p, nsplit, 0, eself.p, d_tau, d_E);
+    EB_LAUNCH_CHECK();
   }
-  k_stress_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, part.p, nsplit, bary, eself.p, d_tau, d_E);
-  EB_LAUNCH_CHECK();
 }
 
 void qoi_targets(State& s, const double* d_den, long long ntar, const double* d_xt, const double* d_yt, double* d_u,

@@ -95,6 +95,12 @@ k_tl_atau(int n, const double* __restrict__ tau, const double* __restrict__ gker
   if (threadIdx.x == 0) matau[b] = s / n;
 }
 
+// d = x - d (the density increment over the previous step), in place.
+__global__ void k_lw_delta(long long n, const double* __restrict__ x, double* __restrict__ d) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) d[i] = x[i] - d[i];
+}
+
 // xyrot (DensityStress.jl:40): (x, y) -> (-y, x), in place.
 __global__ void k_tl_xyrot(long long nb, double* __restrict__ xx, double* __restrict__ yy) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -276,8 +282,11 @@ struct TL {
   // state buffers: 0 = thld0, 1 = thld05, 2 = output
   DBuf<double> th[3], len[3], xsm[3], ysm[3], mat[2];
   DBuf<double> mterm, nterm, xsd, ysd, atau, tau, xx, yy, tmp;
-  DBuf<double> den[2];
+  DBuf<double> den[2], den_prev;
   long long den_ntot[2] = {-1, -1};
+  // per stage: encoding of the last density increment (learned guess input)
+  DBuf<float> hist[2];
+  bool hist_valid[2] = {false, false};
   DBuf<int> flag, map;
   erosion_step_stats stats{};
 };
@@ -390,10 +399,16 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   const long long ntot = s.pr.ntot;
   double* den = T.den[k].ensure(ntot);
   const bool have_prev = sp.warm_start && T.den_ntot[k] == ntot;
-  if (!have_prev) EB_CK(cudaMemsetAsync(den, 0, ntot * sizeof(double), s.st));
+  if (!have_prev) {
+    EB_CK(cudaMemsetAsync(den, 0, ntot * sizeof(double), s.st));
+    T.hist_valid[k] = false;
+  } else {
+    EB_CK(cudaMemcpyAsync(T.den_prev.ensure(ntot), den, ntot * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+  }
   double* rhs = s.d_rhs.ensure(ntot);
   build_rhs(s, rhs);
-  const bool zero = choose_initial_guess(s, rhs, den, have_prev, sp.warm_start == 2);
+  const bool zero = choose_initial_guess(s, rhs, den, have_prev, sp.warm_start == 2,
+                                         T.hist_valid[k] ? T.hist[k].p : nullptr);
   T.stats.guess_used[k] = s.stats.guess_used;
   T.stats.guess_residual[k] = s.stats.guess_used >= 0 ? s.stats.guess_residual[s.stats.guess_used] : -1;
   long long it = 0;
@@ -404,6 +419,13 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   T.stats.matvecs_fp32[k] = s.stats.matvecs_fp32 - mv32;
   if (rc == EROSION_BREAKDOWN) throw Error(EROSION_BREAKDOWN, "GMRES stalled inside the time step");
   T.den_ntot[k] = ntot;
+  if (have_prev && sp.warm_start == 2) {
+    // encoding of this step's increment: the next step's network input
+    k_lw_delta<<<nblk(ntot, 256), 256, 0, s.st>>>(ntot, den, T.den_prev.p);
+    EB_LAUNCH_CHECK();
+    lw_encode_current(s, T.den_prev.p, T.hist[k].ensure((size_t)M * lw_out_width()));
+    T.hist_valid[k] = true;
+  }
   *iters = it;
   *resid = est;
   EB_CK(cudaEventRecord(ev[1], s.st));
@@ -471,6 +493,7 @@ static int delete_and_compact(State& s, TL& T, int M, int n, double dt1, const d
   }
   EB_CK(cudaStreamSynchronize(s.st));
   T.den_ntot[0] = T.den_ntot[1] = -1;   // body count changed: no warm start
+  T.hist_valid[0] = T.hist_valid[1] = false;
   return Mn;
 }
 
@@ -731,6 +754,19 @@ int erosion_drag(const erosion_params* p, int64_t npts, int64_t nbods, int64_t n
     for (int bb = 0; bb < M; ++bb)
       for (int q = 0; q < 4; ++q) drag[q] += per[4 * (size_t)bb + q];
     if (drag_bodies) std::copy(per.begin(), per.end(), drag_bodies);
+    return EROSION_OK;
+  });
+}
+
+int erosion_get_step_density(int32_t stage, double* density, int64_t capacity) {
+  return guarded3([&](State& s) {
+    TL& T = tl();
+    if (stage < 0 || stage > 1 || !density) throw Error(EROSION_BAD_INPUT, "stage must be 0 or 1");
+    const long long n = T.den_ntot[stage];
+    if (n <= 0) throw Error(EROSION_BAD_INPUT, "no solved density of that stage since the last body-count change");
+    if (capacity < n) throw Error(EROSION_BAD_INPUT, "density capacity below the stage's unknown count");
+    d2h(density, T.den[stage].p, n, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
   });
 }

@@ -107,7 +107,24 @@ typedef struct {
                            erosion_lw_train) and start GMRES from whichever of
                            {learned, supplied density, zero} has the smallest FP64
                            residual                                               */
-  int32_t reserved[4];
+  int32_t fast_fp64;    /* mixed mode: 1 (default) applies the fast FP64 operator
+                           (far-field reciprocal to ~1e-12 instead of FP64
+                           rounding) while the residual is above relax_tol, 0 the
+                           accurate one; true residuals always use the accurate  */
+  int32_t precond_refresh; /* block preconditioner: 0 or 1 rebuilds the body blocks
+                           at every set-up; k > 1 keeps the previous inverses for up
+                           to k - 1 further set-ups of the same size (consecutive
+                           stages and time steps of an erosion run, whose shapes
+                           change little).  Flexible GMRES meets the same
+                           tolerance with any fixed preconditioner; only the
+                           iteration count can change                            */
+  int32_t stress_all_bary; /* shear stress with ibary = 1: 0 (default) evaluates
+                           another curve by the barycentric formulas only at body
+                           nodes within 12 of its node spacings and by the
+                           trapezoid rule beyond (where the two agree to
+                           rounding); 1 evaluates every pair barycentrically, as
+                           deformation_on_boundary does                          */
+  int32_t reserved[1];
   double relax_tol;     /* mixed mode: GMRES switches to the FP32 far field once its
                            residual estimate is below relax_tol (relative);
                            0 selects the library default                           */
@@ -153,6 +170,9 @@ typedef struct {
                                and the preconditioner                              */
   double ms_precond_setup;  /* device time of the preconditioner's block assembly
                                and inversion within that set-up                    */
+  double ms_far64f;         /* mixed operator: device time of the fast FP64 far-field
+                               launches (pairs per launch: far64_pairs)            */
+  int64_t far64f_launches;  /* their count                                         */
 } erosion_solve_stats;
 
 /* Host-array solve.  density: initial guess in, solution out. */
@@ -200,7 +220,8 @@ void erosion_get_batch_stats(erosion_batch_stats* s);
  * matvec_DLP_fmmbary / matvec_DLP_bary / matvec_DLP depending on ibary, ifmm;
  * precision = 1 applies the mixed-precision operator (FP32 far field from body
  * sources to the nodes of other curves, FP64 elsewhere, the wall's sources
- * included). */
+ * included); precision = 2 the fast FP64 operator of the mixed solve's early
+ * iterations (FP64 with a far-field reciprocal good to ~1e-12). */
 int erosion_matvec(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                    const double* xx, const double* yy, const double* density, double* vel);
 
@@ -342,6 +363,13 @@ int erosion_rk2_step_device(const erosion_params* p, const erosion_step_params* 
 
 void erosion_get_step_stats(erosion_step_stats* s);
 
+/* The density solved in stage `stage` (0 or 1) of the last RK2 step (host
+ * array of at least 2*npts*nbods + 3*nbods + 2*nouter entries, the body count
+ * after that stage's deletions).  Stage 0 is solved on the state the step
+ * started from.  EROSION_BAD_INPUT when there is none (no step yet, or the
+ * body count changed after the solve). */
+int erosion_get_step_density(int32_t stage, double* density, int64_t capacity);
+
 /* Drag on the bodies of a theta-L state: replaces drag (PostProcess.jl:131-162)
  * with the shear stress and pressure it calls (compute_stress,
  * compute_pressure: computeshearstress_/computepressure_ semantics with
@@ -380,33 +408,46 @@ double erosion_peak_tflops(int32_t precision);
 
 /* Far-field launch shapes (extended API; the reference's FMM has no
  * counterpart).  Each far-field kernel has a list of candidate CTA shapes
- * (threads per CTA x targets per thread); by default an autotuner times
- * every candidate on the geometry at hand the first time a problem of that
- * size is set up (problems above 2e8 node pairs) and keeps the fastest.
+ * (threads per CTA x targets per thread x variant); by default an autotuner
+ * times every candidate on the geometry at hand the first time a problem of
+ * that size is set up (problems above 2e8 node pairs) and keeps the fastest.
  * erosion_set_far_shape(kind, shape) forces candidate 'shape' (kind 0 = the
- * FP64 kernel, 1 = the FP32 kernel) from the next set-up on; shape = -1
+ * accurate FP64 kernel, 1 = the FP32 kernel, 2 = the fast FP64 kernel of the
+ * mixed solve's early iterations) from the next set-up on; shape = -1
  * returns to the autotuner.  Returns EROSION_BAD_INPUT for an unknown kind
  * or shape. */
 int erosion_set_far_shape(int32_t kind, int32_t shape);
 
-/* The shapes in use: shape[kind] = candidate index; desc[12*kind + 3*i ..] =
- * (threads, targets per thread, variant: for the FP64 kernel the reciprocal,
- * 0 division or 1 Newton-Raphson from the FP32 estimate; for the FP32 kernel
- * the unroll factor of the source loop) of candidate i (num_shapes[kind] of them, at most 4,
- * capacity 24 entries); ms[8*kind + i] = the autotuner's time of candidate i
- * in milliseconds (0 when not timed).  Any pointer may be NULL. */
+/* The shapes in use: shape[kind] = candidate index (3 kinds); desc[12*kind +
+ * 3*i ..] = (threads, targets per thread, variant) of candidate i
+ * (num_shapes[kind] of them, at most 4; capacity 36 entries).  The variant
+ * is, for the FP64 kernels, the reciprocal: 1 FP32 estimate + 2
+ * Newton-Raphson steps, 3 FP64 estimate + 2 steps (accurate kind), 2 FP32
+ * estimate + 1 step, 4 FP64 estimate + 1 step (fast kind); for the FP32
+ * kernel the unroll factor of the source loop.  ms[8*kind + i] = the
+ * autotuner's time of candidate i in milliseconds (0 when not timed;
+ * capacity 24).  Any pointer may be NULL. */
 int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* num_shapes);
 
 /* ------------------------------------------------------------------------
  * Learned initial guess (no counterpart in the reference).  A network of
- * 64 -> 256 -> 256 -> 256 -> 37 (GELU, BF16 weights, FP32 accumulation)
- * maps per-body geometry features to the body's density (Fourier modes -8..8
- * scaled by the body radius) and its stokeslet/rotlet strengths.
+ * 105 -> 256 -> 256 -> 256 -> 37 (GELU, BF16 weights, FP32 accumulation)
+ * maps per-body geometry features (68: 32 Fourier shape coefficients, 4
+ * position/size terms, 4 per nearest neighbour for 8 neighbours) and the
+ * encoding of the body's density increment over the previous time step (37)
+ * to the encoding of its increment over the current step.  The encoding of
+ * a density is its Fourier modes -8..8 scaled by the body radius and its
+ * stokeslet/rotlet strengths (linear in the density).  In an erosion step
+ * with warm_start = 2 the guess is the previous step's density plus the
+ * decoded prediction, used when its FP64 residual beats the previous
+ * density's.
  * ------------------------------------------------------------------------ */
-/* Per-body features of a geometry: feat[nbods*64]. */
+/* Widths: geometry features (68), network input (105), encoding (37). */
+int erosion_lw_dims(int32_t* geo, int32_t* in, int32_t* out);
+/* Per-body geometry features of a geometry: feat[nbods*68]. */
 int erosion_lw_features(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                         const double* xx, const double* yy, float* feat);
-/* Per-body targets of a solved density: targ[nbods*37]. */
+/* Per-body encoding of a density (or of a density increment): targ[nbods*37]. */
 int erosion_lw_encode(const erosion_params* p, int64_t npts, int64_t nbods, int64_t nouter,
                       const double* xx, const double* yy, const double* density, float* targ);
 /* Density (body entries, wall zero) of per-body targets. */
@@ -421,7 +462,10 @@ int erosion_lw_set_params(const float* in);
  * rows (x, y) used as given (no standardisation); for checking the backward
  * kernels. */
 int erosion_lw_loss_grad(const float* x, const float* y, int64_t nsamples, double* loss, float* grads);
-/* Trains from scratch: standardisation from the data, then mini-batch Adam. */
+/* Trains from scratch on rows feat[nsamples*105] (geometry features, then the
+ * previous increment's encoding) and targ[nsamples*37] (the encoding of the
+ * increment that followed): standardisation from the data, then mini-batch
+ * Adam. */
 int erosion_lw_train(const float* feat, const float* targ, int64_t nsamples, int64_t epochs, int64_t batch,
                      double lr, uint64_t seed, double* final_loss);
 /* Targets predicted by the trained network for raw features. */

@@ -1,5 +1,5 @@
 """TEST INFRASTRUCTURE ONLY — FP64 numpy restatement of the learned-guess
-network (64 -> 256 -> 256 -> 256 -> 37, exact-erf GELU on the hidden layers,
+network (105 -> 256 -> 256 -> 256 -> 37, exact-erf GELU on the hidden layers,
 mean-squared-error loss) used to check the library's forward and backward
 kernels.  The weights are rounded to BF16 (round to nearest even) exactly as
 the library stores them for its products; the biases stay FP32."""
@@ -9,7 +9,7 @@ import math
 
 import numpy as np
 
-LAYERS = [(64, 256), (256, 256), (256, 256), (256, 37)]
+LAYERS = [(105, 256), (256, 256), (256, 256), (256, 37)]
 
 
 def bf16(a: np.ndarray) -> np.ndarray:

@@ -1,5 +1,6 @@
 """Far-field launch shapes: every candidate the autotuner may pick computes
-the same operator (FP64 shapes, either reciprocal, to 1e-11 of the oracle;
+the same operator (accurate FP64 shapes, either reciprocal, to 1e-11 of the
+oracle; fast FP64 shapes to 1e-10;
 FP32 shapes to 1e-5 of the FP64 operator and to 1e-6 of each other — the
 split-K grouping of the tiles differs between shapes), and the autotuner
 times every candidate on a problem large enough to tune."""
@@ -18,8 +19,8 @@ def rel(a, b):
 @pytest.fixture
 def auto_shapes(lib):
     yield
-    assert lib.erosion_set_far_shape(0, -1) == 0
-    assert lib.erosion_set_far_shape(1, -1) == 0
+    for kind in (0, 1, 2):
+        assert lib.erosion_set_far_shape(kind, -1) == 0
 
 
 def test_every_shape_computes_the_same_operator(lib, oracle, auto_shapes):
@@ -32,6 +33,10 @@ def test_every_shape_computes_the_same_operator(lib, oracle, auto_shapes):
         assert lib.erosion_set_far_shape(0, i) == 0
         assert rel(stokes.matvec(g, den, precision=0), ref) < 1e-11, i
         assert _lib.far_shapes()["fp64"]["index"] == i
+    for i in range(len(num["fp64_fast"]["tuned_ms"])):   # the fast FP64 operator (reciprocal to ~1e-12)
+        assert lib.erosion_set_far_shape(2, i) == 0
+        assert rel(stokes.matvec(g, den, precision=2), ref) < 1e-10, i
+        assert _lib.far_shapes()["fp64_fast"]["index"] == i
     for i in range(len(num["fp32"]["tuned_ms"])):
         assert lib.erosion_set_far_shape(1, i) == 0
         a = stokes.matvec(g, den, precision=1)
@@ -44,7 +49,8 @@ def test_every_shape_computes_the_same_operator(lib, oracle, auto_shapes):
 
 def test_unknown_shape_rejected(lib):
     assert lib.erosion_set_far_shape(1, 17) == _lib.EROSION_BAD_INPUT
-    assert lib.erosion_set_far_shape(2, 0) == _lib.EROSION_BAD_INPUT
+    assert lib.erosion_set_far_shape(3, 0) == _lib.EROSION_BAD_INPUT
+    assert lib.erosion_set_far_shape(-1, 0) == _lib.EROSION_BAD_INPUT
 
 
 def test_autotuner_times_every_candidate(lib, auto_shapes):
@@ -52,7 +58,7 @@ def test_autotuner_times_every_candidate(lib, auto_shapes):
     den = np.random.default_rng(1).standard_normal(g.ntot)
     stokes.matvec(g, den, precision=1)
     sh = _lib.far_shapes()
-    for kind in ("fp64", "fp32"):
+    for kind in ("fp64", "fp32", "fp64_fast"):
         ms = sh[kind]["tuned_ms"]
         assert all(v > 0 for v in ms.values()), (kind, ms)
         best = min(ms, key=ms.get)

@@ -1,12 +1,12 @@
 """The learned initial guess: the backward kernels against the FP64 numpy
 oracle, the density encoding, training on the solver's own densities, and
-what the trained network gains over a zero initial guess."""
+what the trained network gains over the previous-step initial guess."""
 import ctypes
 
 import numpy as np
 import pytest
 
-from erosion_b200 import _lib, geometry as G, stokes
+from erosion_b200 import _lib, geometry as G, learned, stokes
 from oracle import mlp_oracle
 
 pytestmark = pytest.mark.gpu
@@ -24,8 +24,8 @@ def test_gradients_match_cpu_oracle(lib):
     params = np.zeros(npar, np.float32)
     assert lib.erosion_lw_get_params(fptr(params)) == 0
     rng = np.random.default_rng(0)
-    x = rng.standard_normal((8, 64)).astype(np.float32)
-    y = rng.standard_normal((8, 37)).astype(np.float32)
+    x = rng.standard_normal((8, mlp_oracle.LAYERS[0][0])).astype(np.float32)
+    y = rng.standard_normal((8, mlp_oracle.LAYERS[-1][1])).astype(np.float32)
     loss = ctypes.c_double()
     grads = np.zeros(npar, np.float32)
     assert lib.erosion_lw_loss_grad(fptr(x), fptr(y), 8, ctypes.byref(loss), fptr(grads)) == 0
@@ -39,25 +39,6 @@ def test_gradients_match_cpu_oracle(lib):
         a, b = grads[o:o + k], g_ref[o:o + k]
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
         o += k
-
-
-def _training_set(seeds, n=128, nout=1024):
-    feats, targs, geos = [], [], []
-    for s in seeds:
-        g = G.workload("c1", seed=s)
-        den, nits, st = stokes.solve(g, precond=1)
-        p = stokes.params_for(g)
-        f = np.zeros((g.M, 64), np.float32)
-        t = np.zeros((g.M, 37), np.float32)
-        xx, yy = g.xx, g.yy
-        assert _lib.load().erosion_lw_features(ctypes.byref(p), g.n, g.M, g.nout, _lib.ptr(xx), _lib.ptr(yy),
-                                               fptr(f)) == 0
-        assert _lib.load().erosion_lw_encode(ctypes.byref(p), g.n, g.M, g.nout, _lib.ptr(xx), _lib.ptr(yy),
-                                             _lib.ptr(den), fptr(t)) == 0
-        feats.append(f)
-        targs.append(t)
-        geos.append((g, den, nits))
-    return np.concatenate(feats), np.concatenate(targs), geos
 
 
 def test_encode_decode_round_trip(lib):
@@ -77,33 +58,62 @@ def test_encode_decode_round_trip(lib):
     assert np.allclose(back[-3 * g.M:], den[-3 * g.M:], rtol=1e-6, atol=1e-6 * np.abs(den[-3 * g.M:]).max())
 
 
+def _state(seed):
+    g = G.workload("c1", seed=seed)
+    th, ln, xs, ys = G.to_thetalen(g)
+    return g, th.copy(), ln.copy(), xs.copy(), ys.copy()
+
+
+def _step_params(g, warm_start, dt=1e-5):
+    sp = _lib.StepParams()
+    _lib.load().erosion_default_step_params(ctypes.byref(sp), g.n)
+    sp.dt = dt
+    sp.fixpdrop = 0
+    sp.warm_start = warm_start
+    return sp
+
+
 def test_training_and_learned_guess_gain(lib):
-    """Trains on the densities of 40 ten-body solves and measures, on five
-    held-out geometries, the learned candidate's initial residual and the GMRES
-    iterations with the learned guess (plus fallback) against a zero guess.
-    The residual-checked fallback guarantees the learned path never starts
-    from a worse guess than the method without it; the measured gain is
-    printed (on this operator the local features do not predict the density
-    accurately enough to beat the zero guess, so the fallback is taken)."""
-    X, Y, _ = _training_set(range(100, 140))
-    loss0 = ctypes.c_double()
-    loss = ctypes.c_double()
-    assert lib.erosion_lw_train(fptr(X), fptr(Y), len(X), 1, 64, 1e-3, 3, ctypes.byref(loss0)) == 0
-    assert lib.erosion_lw_train(fptr(X), fptr(Y), len(X), 300, 64, 1e-3, 3, ctypes.byref(loss)) == 0
-    assert loss.value < 0.5 * loss0.value
-    res_l, it_l, it_0, used = [], [], [], []
-    for s in range(200, 205):   # held-out geometries
-        g = G.workload("c1", seed=s)
-        _, n0, st0 = stokes.solve(g, precond=1)
-        den, nl, stl = stokes.solve(g, precond=1, learned_guess=1)
-        res_l.append(stl["guess_residual"][2])
-        used.append(stl["guess_used"])
-        it_l.append(nl)
-        it_0.append(n0)
-        assert stl["est_residual"] <= 1e-8
-        assert 0 < stl["guess_residual"][2]          # the learned candidate was evaluated
-        if stl["guess_residual"][2] >= 1.0:
-            assert stl["guess_used"] == 0            # ... and rejected when worse than zero
-    print(f"training MSE {loss0.value:.3f} -> {loss.value:.3f}; learned-guess residual {np.mean(res_l):.3g} "
-          f"(zero guess 1.0), used {used}; iterations {np.mean(it_l):.1f} vs zero guess {np.mean(it_0):.1f}")
-    assert np.mean(it_l) <= np.mean(it_0) + 2
+    """Trains the increment network on a 40-step erosion run of one ten-body
+    channel (rows: geometry + previous increment -> next increment, from the
+    solver's own densities), then runs a held-out channel for 12 steps with
+    the previous-step guess (warm_start = 1) and with the learned guess
+    (warm_start = 2: previous density plus the predicted increment, used
+    only when its FP64 residual is smaller).  Both reach the tolerance; the
+    learned candidate is evaluated every stage once it has a history, and the
+    measured gain in initial residual and iterations is printed."""
+    g, th, ln, xs, ys = _state(100)
+    p = stokes.params_for(g, precision=1, precond=1)
+    traj = learned.trajectory(p, _step_params(g, 1), g.n, g.nout, th, ln, xs, ys, 40)
+    X, Y = learned.training_rows(p, g.n, g.nout, traj)
+    assert X.shape[1] == learned.dims()[1] and len(X) >= 300
+    loss0 = learned.train(X, Y, epochs=1)
+    loss = learned.train(X, Y, epochs=300)
+    assert loss < 0.5 * loss0
+    runs = {}
+    for ws in (1, 2):
+        g2, th, ln, xs, ys = _state(200)
+        sp = _step_params(g2, ws)
+        nb = np.array([g2.M], np.int64)
+        t = np.zeros(1)
+        dele = np.zeros(g2.M, np.int64)
+        its, res, used = [], [], []
+        for k in range(12):
+            rc = lib.erosion_rk2_step(ctypes.byref(p), ctypes.byref(sp), g2.n, nb.ctypes.data_as(_lib.PI64), g2.nout,
+                                      _lib.ptr(th), _lib.ptr(ln), _lib.ptr(xs), _lib.ptr(ys),
+                                      t.ctypes.data_as(_lib.PD), dele.ctypes.data_as(_lib.PI64))
+            assert rc == 0
+            st = _lib.StepStats()
+            lib.erosion_get_step_stats(ctypes.byref(st))
+            d = st.as_dict()
+            assert d["max_residual"] <= 2e-8
+            if k >= 2:   # the learned candidate needs the previous increment
+                its.append(sum(d["gmres_iterations"]))
+                res.append(np.mean(d["guess_residual"]))
+                used.append(d["guess_used"])
+        runs[ws] = (np.mean(its), np.mean(res), used)
+    assert all(u in (1, 2) for pair in runs[2][2] for u in pair)
+    print(f"training MSE {loss0:.3f} -> {loss:.3f}; initial residual previous-step {runs[1][1]:.3g} vs learned "
+          f"{runs[2][1]:.3g}; iterations per step {runs[1][0]:.1f} vs {runs[2][0]:.1f}; learned used "
+          f"{sum(u == 2 for pair in runs[2][2] for u in pair)} of {2 * len(runs[2][2])} stages")
+    assert runs[2][0] <= runs[1][0] + 2

@@ -118,3 +118,18 @@ def test_boundary_pressure_manufactured(lib):
     den, _, _ = stokes.solve(g, tol=1e-13, rhs_mode=1)
     exact = (g.xx + 2 * g.yy) / (2 * np.pi * (g.xx ** 2 + g.yy ** 2))
     assert np.abs(stokes.pressure(g, den) - exact).max() < 1e-9 * np.abs(exact).max()
+
+
+@pytest.mark.parametrize("name,seed", [("c1", 2), ("c2", 0)])
+def test_hybrid_stress_equals_all_barycentric(lib, name, seed):
+    """The default shear stress (barycentric within 12 node spacings of a
+    source curve, trapezoid rule beyond) against the reference's evaluation
+    of every pair by the barycentric formulas, on a random density (content
+    up to the Nyquist mode: the hardest case for the trapezoid rule)."""
+    g = G.workload(name, seed=seed)
+    den = np.random.default_rng(5).standard_normal(g.ntot)
+    tau, E = stokes.shear_stress(g, den)
+    tau_b, E_b = stokes.shear_stress(g, den, stress_all_bary=1)
+    assert rel(tau, tau_b) < 1e-10
+    for q in range(3):
+        assert rel(E[q], E_b[q]) < 1e-10

@@ -232,8 +232,8 @@ def test_mlp_oracle_gradient_by_finite_differences(monkeypatch):
         params[o:o + ni * no] = rng.standard_normal(ni * no) * np.sqrt(2.0 / ni)
         params[o + ni * no:o + ni * no + no] = 0.1 * rng.standard_normal(no)
         o += ni * no + no
-    x = rng.standard_normal((4, 64))
-    y = rng.standard_normal((4, 37))
+    x = rng.standard_normal((4, mlp_oracle.LAYERS[0][0]))
+    y = rng.standard_normal((4, mlp_oracle.LAYERS[-1][1]))
     _, g = mlp_oracle.loss_and_grad(params, x, y)
     idx = rng.choice(npar, 24, replace=False)
     h = 1e-6
