@@ -96,6 +96,11 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ensemble", type=int, default=64, help="geometries of the c4 ensemble")
+    ap.add_argument("--c5-steps", type=int, default=40,
+                    help="c5: target number of steps for 50%% of the body area to erode (sets dt)")
+    ap.add_argument("--c5-max-steps", type=int, default=120, help="c5: cap on the steps of each run")
+    ap.add_argument("--train-steps", type=int, default=15,
+                    help="c5: steps of the 400-body run whose first-stage densities train the network")
     return ap.parse_args(argv)
 
 
@@ -370,6 +375,122 @@ def run_ensemble(args, world, rank, local, dist):
                         "entry_point": "erosion_solve_batch (host arrays)"},
                 "clocks": clk.summary()}
         print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+def run_learned(args, world, rank, local, dist):
+    """The learned warm start (workload c5): trains the increment network on
+    the first-stage densities of a 400-body run (c3 shapes, a different seed),
+    then erodes a 200-body, 256-node channel until half of its body area is
+    gone, once with the previous step's density as the GMRES initial guess
+    (warm_start = 1) and once with the learned guess (warm_start = 2), both
+    mixed precision + block preconditioner to 1e-8.  dt is set from a first
+    step so that the run takes about --c5-steps steps.  value = erosion steps/s
+    of the learned run (device time of its steps); the line reports both runs'
+    GMRES iterations and time per step."""
+    import torch
+    from erosion_b200 import _lib, geometry as G, learned
+    L = _lib.load()
+    stream = torch.cuda.ExternalStream(L.erosion_stream(), device=torch.device("cuda", local))
+    g5 = G.workload("c5", seed=args.seed + rank)
+    n, nout = g5.n, g5.nout
+    p = _lib.default_params(wall=tuple(g5.wall), ibc=g5.ibc, precision=args.precision, precond=args.precond)
+
+    def sparams(dt, ws):
+        sp = _lib.StepParams()
+        L.erosion_default_step_params(ctypes.byref(sp), n)
+        sp.dt = dt
+        sp.fixpdrop = 0
+        sp.warm_start = ws
+        return sp
+
+    init = [a.copy() for a in G.to_thetalen(g5)]
+    A0 = float(learned.areas(n, *init).sum())
+    # dt from the area lost over one probe step
+    th, ln, xs, ys = [a.copy() for a in init]
+    nb = np.array([g5.M], np.int64)
+    t = np.zeros(1)
+    dele = np.zeros(g5.M, np.int64)
+    dt0 = 1e-6
+    _lib.check(L.erosion_rk2_step(ctypes.byref(p), ctypes.byref(sparams(dt0, 0)), n, nb.ctypes.data_as(_lib.PI64),
+                                  nout, _lib.ptr(th), _lib.ptr(ln), _lib.ptr(xs), _lib.ptr(ys),
+                                  t.ctypes.data_as(_lib.PD), dele.ctypes.data_as(_lib.PI64)), (0, 1))
+    rate = max((A0 - float(learned.areas(n, th[: int(nb[0]) * n], ln[: nb[0]], xs[: nb[0]], ys[: nb[0]]).sum()))
+               / dt0, 1e-12)
+    dt = 0.5 * A0 / rate / max(args.c5_steps, 1)
+    # training set: first-stage densities of a 400-body run at the same dt
+    g3 = G.workload("c3", seed=args.seed + 1)
+    t3 = [a.copy() for a in G.to_thetalen(g3)]
+    t_train0 = time.perf_counter()
+    traj = learned.trajectory(p, sparams(dt, 1), g3.n, g3.nout, *t3, args.train_steps)
+    X, Y = learned.training_rows(p, g3.n, g3.nout, traj)
+    loss0 = learned.train(X, Y, epochs=1)
+    loss = learned.train(X, Y, epochs=300)
+    t_train = time.perf_counter() - t_train0
+    runs = {}
+    for ws in (1, 2):
+        th, ln, xs, ys = [a.copy() for a in init]
+        nb = np.array([g5.M], np.int64)
+        t = np.zeros(1)
+        dele = np.zeros(g5.M, np.int64)
+        sp = sparams(dt, ws)
+        rec = {"iterations": [], "ms": [], "guess_used": [], "guess_residual": [], "bodies": [], "area_frac": []}
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        area = A0
+        while area > 0.5 * A0 and len(rec["ms"]) < args.c5_max_steps and int(nb[0]) > 0:
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                rc = L.erosion_rk2_step(ctypes.byref(p), ctypes.byref(sp), n, nb.ctypes.data_as(_lib.PI64), nout,
+                                        _lib.ptr(th), _lib.ptr(ln), _lib.ptr(xs), _lib.ptr(ys),
+                                        t.ctypes.data_as(_lib.PD), dele.ctypes.data_as(_lib.PI64))
+                e1.record(stream)
+            torch.cuda.synchronize()
+            _lib.check(rc, (_lib.EROSION_OK, _lib.EROSION_MAXITER))
+            st = _lib.StepStats()
+            L.erosion_get_step_stats(ctypes.byref(st))
+            d = st.as_dict()
+            M = int(nb[0])
+            area = float(learned.areas(n, th[: M * n], ln[:M], xs[:M], ys[:M]).sum()) if M else 0.0
+            rec["iterations"].append(d["gmres_iterations"])
+            rec["ms"].append(e0.elapsed_time(e1))
+            rec["guess_used"].append(d["guess_used"])
+            rec["guess_residual"].append(d["guess_residual"])
+            rec["bodies"].append(M)
+            rec["area_frac"].append(area / A0)
+        steps = len(rec["ms"])
+        tot_ms = float(np.sum(rec["ms"]))
+        its = [sum(i) for i in rec["iterations"]]
+        runs[ws] = {"steps": steps, "steps_per_s": steps / (tot_ms * 1e-3), "ms_per_step": tot_ms / steps,
+                    "gmres_iterations_per_step": float(np.mean(its)),
+                    "gmres_iterations_per_step_after_2": float(np.mean(its[2:])) if steps > 2 else None,
+                    "ms_per_solve": tot_ms / (2 * steps),
+                    "final_area_frac": rec["area_frac"][-1], "bodies_end": rec["bodies"][-1], "record": rec}
+    if rank == 0:
+        prev, lrn = runs[1], runs[2]
+        used = [u for pair in lrn["record"]["guess_used"] for u in pair]
+        line = {"metric": "erosion steps/s at 1e-8 residual, 200-body run to 50% eroded area (learned vs "
+                          "previous-step warm start)",
+                "value": lrn["steps_per_s"], "unit": "steps/s", "n_gpus": world, "steps": lrn["steps"],
+                "warmup": 0, "ms_per_step": lrn["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+                "config": {"workload": f"c5: {WORKLOADS['c5']['desc']}", "bodies": g5.M, "nodes_per_body": n,
+                           "wall_nodes": nout, "dt": dt, "dt_rule": f"half the body area in about "
+                                                                      f"{args.c5_steps} steps (from one probe step)",
+                           "tol": 1e-8, "precision": "mixed" if args.precision else "fp64",
+                           "precond": "block Gauss-Seidel" if args.precond else "none",
+                           "training": {"rows": int(len(X)), "source": f"first-stage densities of "
+                                                                       f"{args.train_steps} steps of a 400-body "
+                                                                       f"run (c3 shapes, seed {args.seed + 1})",
+                                        "epochs": 300, "mse_first_epoch": loss0, "mse_last_epoch": loss,
+                                        "seconds": t_train}},
+                "previous_step": {k: v for k, v in prev.items() if k != "record"},
+                "learned": {k: v for k, v in lrn.items() if k != "record"},
+                "learned_guess_used_stages": int(sum(u == 2 for u in used)), "stages": len(used),
+                "gain": {"iterations_per_step": prev["gmres_iterations_per_step"] - lrn["gmres_iterations_per_step"],
+                         "time_per_step_ratio": prev["ms_per_step"] / lrn["ms_per_step"]},
+                "records": {"previous_step": prev["record"], "learned": lrn["record"]}}
+        print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -653,6 +774,8 @@ def main(argv=None):
         torch.cuda.set_device(local)
         if args.workload == "c4":
             run_ensemble(args, world, rank, local, dist)
+        elif args.workload == "c5":
+            run_learned(args, world, rank, local, dist)
         else:
             run_steps(args, world, rank, local, dist)
     finally:

@@ -111,7 +111,8 @@ class BatchStats(ctypes.Structure):
     _fields_ = [("geometries", c_int64), ("rounds", c_int64), ("iterations", c_int64), ("graph_captures", c_int64),
                 ("ms_total", c_double), ("pairs64_per_round", c_double), ("pairs32_per_round", c_double),
                 ("pairs64_total", c_double), ("pairs32_total", c_double), ("max_true_residual", c_double),
-                ("shape64", c_int64), ("shape32", c_int64), ("tune_ms", ctypes.c_float * 8)]
+                ("shape64", c_int64), ("shape32", c_int64), ("tune_ms", ctypes.c_float * 8),
+                ("setup_host_ms", c_double)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}

@@ -24,6 +24,9 @@
 #include <vector>
 
 #include "state.h"
+#include <chrono>
+#include <exception>
+#include <thread>
 #include "kernels.cuh"
 
 namespace eb {
@@ -227,8 +230,8 @@ void launch_batch32(Batch& B, int shape, int njobs, long long items, cudaStream_
   switch (shape) {
     EB_B32(0, 256, 4, 2)
     EB_B32(1, 256, 4, 4)
-    EB_B32(2, 128, 4, 4)
-    EB_B32(3, 128, 4, 2)
+    EB_B32(2, 256, 2, 2)
+    EB_B32(3, 256, 2, 4)
     default: throw Error(EROSION_BAD_INPUT, "unknown FP32 batch shape");
   }
 #undef EB_B32
@@ -239,7 +242,8 @@ static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Sha
               kFar64Shapes[1].nt == 128 && kFar64Shapes[1].tpt == 4 && kFar64Shapes[1].rcp == 1 &&
               kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 2 && kFar64Shapes[2].rcp == 3 &&
               kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 3 &&
-              kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].rcp == 4,
+              kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
+              kFar32Shapes[2].nt == 256 && kFar32Shapes[2].tpt == 2 && kFar32Shapes[3].rcp == 4,
               "launch_batch shape tables");
 
 // Chooses the ensemble launch shapes by timing each candidate on the jobs of
@@ -251,8 +255,8 @@ void occupancy(Batch& B) {
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[3], k_far64_batch<128, 4, 3>, 128, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[0], k_far32_batch<256, 4, 2>, 256, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[1], k_far32_batch<256, 4, 4>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[2], k_far32_batch<128, 4, 4>, 128, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[3], k_far32_batch<128, 4, 2>, 128, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[2], k_far32_batch<256, 2, 2>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[3], k_far32_batch<256, 2, 4>, 256, 0));
 }
 
 void tune_batch(Batch& B, double pairs_total) {
@@ -603,18 +607,33 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
     }
     cudaStream_t st = lib.st;
     EB_CK(cudaEventRecord(B.a, st));
-    // set-up: geometry, near lists, tiles, preconditioner, right-hand side
-    size_t node_off = 0, den_off = 0;
-    double pairs_total = 0;
+    // set-up: geometry, near lists, tiles, preconditioner, right-hand side.
+    // Each member works on its own stream and buffers, so the members' set-ups
+    // (host near-list construction included) run on a pool of host threads.
+    std::vector<size_t> node_offs(nbatch), den_offs(nbatch);
+    {
+      size_t node_off = 0, den_off = 0;
+      for (int g = 0; g < nbatch; ++g) {
+        if (npts[g] < 0 || nbods[g] < 0 || nouter[g] < 0) throw Error(EROSION_BAD_INPUT, "negative sizes");
+        node_offs[g] = node_off;
+        den_offs[g] = den_off;
+        node_off += (size_t)npts[g] * nbods[g];
+        den_off += 2 * (size_t)nouter[g] + 2 * (size_t)npts[g] * nbods[g] + 3 * (size_t)nbods[g];
+      }
+    }
     for (int g = 0; g < nbatch; ++g) {
       Member& mb = B.m[g];
       mb.s = std::make_unique<State>();
-      State& s = *mb.s;
-      init_member_state(s, lib);
+      init_member_state(*mb.s, lib);
       EB_CK(cudaStreamCreateWithFlags(&mb.side, cudaStreamNonBlocking));
       EB_CK(cudaEventCreateWithFlags(&mb.ev_pre, cudaEventDisableTiming));
       EB_CK(cudaEventCreateWithFlags(&mb.ev_post, cudaEventDisableTiming));
-      s.st = mb.side;
+      mb.s->st = mb.side;
+    }
+    const auto t_setup = std::chrono::steady_clock::now();
+    auto setup_member = [&](int g) {
+      Member& mb = B.m[g];
+      State& s = *mb.s;
       // the ensemble's far field runs in the ensemble's own launch shapes
       // (tune_batch), so the members skip the per-geometry timing
       s.force_shape[0] = 0;
@@ -622,14 +641,12 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       s.force_shape[2] = 0;
       Problem pr;
       pr.P = P;
-      if (npts[g] < 0 || nbods[g] < 0 || nouter[g] < 0) throw Error(EROSION_BAD_INPUT, "negative sizes");
       pr.n = (int)npts[g]; pr.M = (int)nbods[g]; pr.nout = (int)nouter[g];
       const size_t nb = (size_t)pr.n * pr.M;
       double* dx = s.d_xx.ensure(std::max<size_t>(nb, 1));
       double* dy = s.d_yy.ensure(std::max<size_t>(nb, 1));
-      h2d(dx, xx + node_off, nb, s.st);
-      h2d(dy, yy + node_off, nb, s.st);
-      node_off += nb;
+      h2d(dx, xx + node_offs[g], nb, s.st);
+      h2d(dy, yy + node_offs[g], nb, s.st);
       setup_problem(s, pr, dx, dy);
       mb.ntot = s.pr.ntot;
       mb.ldv = (mb.ntot + 31) & ~31LL;
@@ -640,10 +657,9 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
       mb.hn.ensure(1); mb.scal.ensure(4); mb.kdev.ensure(1); mb.stdev.ensure(1);
       mb.vcap = mb.zcap = mb.rcols = mb.partcap = 0;
       s.V.release(); s.Z.release();
-      h2d(mb.x.p, density + den_off, (size_t)mb.ntot, s.st);
+      h2d(mb.x.p, density + den_offs[g], (size_t)mb.ntot, s.st);
       bool zero = true;
-      for (long long i = 0; i < mb.ntot && zero; ++i) zero = density[den_off + i] == 0.0;
-      den_off += mb.ntot;
+      for (long long i = 0; i < mb.ntot && zero; ++i) zero = density[den_offs[g] + i] == 0.0;
       build_rhs(s, mb.b.p);
       mb.bnrm = device_norm(s, mb.b.p, mb.ntot);
       if (mb.bnrm == 0.0) throw Error(EROSION_BAD_INPUT, "erosion_solve_batch: zero right-hand side");
@@ -657,10 +673,30 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
         k_bminus<<<nblk(mb.ntot, 256), 256, 0, s.st>>>(mb.b.p, mb.r.p, mb.ntot);
         EB_LAUNCH_CHECK();
       }
-      pairs_total += (double)s.far64_pairs;
       if (!start_cycle(mb)) finish_cycle(mb, EROSION_OK, P.tol);
       EB_CK(cudaStreamSynchronize(s.st));
+    };
+    {
+      const int nthr = std::max(1, std::min<int>(nbatch, std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+      std::vector<std::thread> pool;
+      std::vector<std::exception_ptr> errs(nthr);
+      for (int t = 0; t < nthr; ++t)
+        pool.emplace_back([&, t]() {
+          try {
+            EB_CK(cudaSetDevice(lib.device));
+            for (int g = t; g < nbatch; g += nthr) setup_member(g);
+          } catch (...) {
+            errs[t] = std::current_exception();
+          }
+        });
+      for (auto& th : pool) th.join();
+      for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
     }
+    B.stats.setup_host_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
+    double pairs_total = 0;
+    for (int g = 0; g < nbatch; ++g) pairs_total += (double)B.m[g].s->far64_pairs;
     if (!B.ev_far) {
       EB_CK(cudaEventCreateWithFlags(&B.ev_far, cudaEventDisableTiming));
       EB_CK(cudaEventCreateWithFlags(&B.ev_start, cudaEventDisableTiming));
@@ -718,11 +754,9 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
     EB_CK(cudaEventElapsedTime(&ms, B.a, B.b));
     B.stats.ms_total = ms;
     int worst = EROSION_OK;
-    den_off = 0;
     for (int g = 0; g < nbatch; ++g) {
       Member& mb = B.m[g];
-      d2h(density + den_off, mb.x.p, (size_t)mb.ntot, st);
-      den_off += mb.ntot;
+      d2h(density + den_offs[g], mb.x.p, (size_t)mb.ntot, st);
       nits[g] = mb.total;
       B.stats.iterations += mb.total;
       if (mb.status != EROSION_OK && worst == EROSION_OK) worst = mb.status;
@@ -737,6 +771,11 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
     destroy_graph(batch());
     set_status(e.code, e.what());
     return e.code;
+  } catch (const std::exception& e) {
+    if (lib.st) cudaStreamSynchronize(lib.st);
+    destroy_graph(batch());
+    set_status(EROSION_CUDA_ERROR, e.what());
+    return EROSION_CUDA_ERROR;
   }
 }
 

@@ -13,7 +13,7 @@ State& state() {
   return s;
 }
 
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 
 thread_local int t_status = EROSION_OK;
 thread_local std::string t_err;
@@ -266,8 +266,8 @@ static_assert(kFar64FastShapes[0].nt == 256 && kFar64FastShapes[0].tpt == 2 && k
               "launch_far's fast FP64 cases");
 static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[0].rcp == 2 &&
               kFar32Shapes[1].nt == 256 && kFar32Shapes[1].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
-              kFar32Shapes[2].nt == 128 && kFar32Shapes[2].tpt == 4 && kFar32Shapes[2].rcp == 4 &&
-              kFar32Shapes[3].nt == 128 && kFar32Shapes[3].tpt == 4 && kFar32Shapes[3].rcp == 2,
+              kFar32Shapes[2].nt == 256 && kFar32Shapes[2].tpt == 2 && kFar32Shapes[2].rcp == 2 &&
+              kFar32Shapes[3].nt == 256 && kFar32Shapes[3].tpt == 2 && kFar32Shapes[3].rcp == 4,
               "launch_far's FP32 cases");
 
 // One far-field launch of the given kind (0 accurate FP64 and 2 fast FP64 on
@@ -300,8 +300,8 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
     switch (shape) {
       EB_FAR32(0, 256, 4, 2)
       EB_FAR32(1, 256, 4, 4)
-      EB_FAR32(2, 128, 4, 4)
-      EB_FAR32(3, 128, 4, 2)
+      EB_FAR32(2, 256, 2, 2)
+      EB_FAR32(3, 256, 2, 4)
       default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
     }
   } else if (kind == 0) {
@@ -1235,7 +1235,7 @@ void* erosion_stream(void) {
   return (void*)s.st;
 }
 
-int64_t erosion_launch_count(void) { return (int64_t)g_launches; }
+int64_t erosion_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int erosion_set_far_shape(int32_t kind, int32_t shape) {
   State& s = state();

@@ -3,6 +3,7 @@
 // channel of the C ABI.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -14,7 +15,7 @@
 
 namespace eb {
 
-extern long long g_launches;
+extern std::atomic<long long> g_launches;
 
 struct Error : std::runtime_error {
   int code;

@@ -212,6 +212,9 @@ typedef struct {
   double max_true_residual;  /* largest final residual over the geometries         */
   int64_t shape64, shape32;  /* ensemble launch shapes (indices as erosion_get_far_shapes) */
   float tune_ms[8];          /* timed candidates: [0..3] FP64, [4..7] FP32 (0 = not timed) */
+  double setup_host_ms;      /* host wall time of the members' set-ups (geometry,
+                                near lists, tiles, preconditioners, initial residuals),
+                                run on a pool of host threads                      */
 } erosion_batch_stats;
 
 void erosion_get_batch_stats(erosion_batch_stats* s);
