@@ -111,7 +111,7 @@ void destroy_graph(Batch& B) {
 FarJob64 job64(State& s, const int* sp, int nsplit, double2* partial, int nt_tpt) {
   FarJob64 J;
   J.G = s.geo();
-  J.ws = s.wrest.p;
+  J.sq = s.sq64.p;
   J.tiles = s.tiles.p;
   J.split_ptr = sp;
   J.mask = s.near.npairs > 0 ? s.near.mask.p : nullptr;
@@ -126,7 +126,7 @@ FarJob64 job64(State& s, const int* sp, int nsplit, double2* partial, int nt_tpt
 FarJob32 job32(State& s, int nt_tpt) {
   FarJob32 J;
   J.N = s.pr.N; J.nout = s.pr.nout; J.n = s.pr.n;
-  J.src = s.src32.p; J.tgt = s.tgt32.p; J.anchor = s.anchor.p; J.tile_c = s.tile_c.p; J.ws32 = s.ws32.p;
+  J.src = s.src32.p; J.tgt = s.tgt32.p; J.anchor = s.anchor.p; J.tile_c = s.tile_c.p; J.sq32 = s.sq32.p;
   J.tiles = s.tiles.p;
   J.split_ptr = s.split_ptr32.p;
   J.mask = s.near.npairs > 0 ? s.near.mask.p : nullptr;
@@ -268,8 +268,8 @@ void tune_batch(Batch& B, double pairs_total) {
   cudaStream_t st = state().st;
   for (auto& mb : B.m) {
     State& s = *mb.s;
-    EB_CK(cudaMemsetAsync(s.ws32.p, 0, sizeof(float2) * s.pr.N, st));
-    EB_CK(cudaMemsetAsync(s.wrest.p, 0, sizeof(double2) * s.pr.N, st));
+    EB_CK(cudaMemsetAsync(s.sq32.p, 0, sizeof(float4) * s.pr.N, st));
+    EB_CK(cudaMemsetAsync(s.sq64.p, 0, sizeof(double4) * s.pr.N, st));
   }
   for (int kind = 0; kind < 2; ++kind) {
     const std::vector<int> key(B.m.size(), kind);

@@ -105,7 +105,8 @@ __global__ void k_body_stats(int n, int nout, const double2* __restrict__ xy, co
 // ---------------------------------------------------------------------------
 // Per-matvec preparation: one CTA per curve.  Writes
 //   ws    = w * sigma               (full strengths: self-curve sums)
-//   wrest = w * (sigma - rigid part) (strengths seen by other curves)
+//   sq64, sq32: the pair tensors (pair_tensor64/32) of the strengths seen by
+//         other curves, v = w * (sigma - rigid part)
 // the constraint rows of every body (:1055-1096) and the wall's integral of
 // sigma.n for the rank-one term (:1107-1111).  The rigid part of a body's
 // density is its speed-weighted projection on the translations and the
@@ -116,9 +117,21 @@ __global__ void k_body_stats(int n, int nout, const double2* __restrict__ xy, co
 // ~lambda/r and ~xi/r^3 into these modes).  The split is made only when the
 // close pairs are masked for the barycentric correction (split_rigid = 1): at a
 // few node spacings the trapezoid rule's error on a rigid mode is ~1e-9.
+// The FP32 far field's source record of a node: the symmetric tensor S with
+// (r.n)(r.v) = r^T S r for the normal n and the weighted strength v,
+// (S_xx, 2 S_xy, S_yy) = (n_x v_x, n_x v_y + n_y v_x, n_y v_y), formed in
+// FP64 and rounded once.
+__device__ __forceinline__ float4 pair_tensor32(double2 nn, double2 v) {
+  return make_float4((float)(nn.x * v.x), (float)(nn.x * v.y + nn.y * v.x), (float)(nn.y * v.y), 0.f);
+}
+
+__device__ __forceinline__ double4 pair_tensor64(double2 nn, double2 v) {
+  return make_double4(nn.x * v.x, nn.x * v.y + nn.y * v.x, nn.y * v.y, 0.0);
+}
+
 __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict__ den,
-                                              double2* __restrict__ ws, double2* __restrict__ wrest,
-                                              float2* __restrict__ ws32, double* __restrict__ vel,
+                                              double2* __restrict__ ws, double4* __restrict__ sq64,
+                                              float4* __restrict__ sq32, double* __restrict__ vel,
                                               double* __restrict__ sigdotn, int split_rigid) {
   __shared__ double sh[32];
   const int c = blockIdx.x;
@@ -131,9 +144,9 @@ __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict
       double wg = G.w[g];
       double2 v = make_double2(wg * sx, wg * sy);
       ws[g] = v;
-      wrest[g] = v;
-      ws32[g] = make_float2((float)v.x, (float)v.y);
       double2 nn = G.nrm[g];
+      sq64[g] = pair_tensor64(nn, v);
+      sq32[g] = pair_tensor32(nn, v);
       a0 += (nn.x * sx + nn.y * sy) * G.sp[g];
     }
     a0 = block_sum<256>(a0, sh);
@@ -190,8 +203,9 @@ __global__ void __launch_bounds__(256) k_prep(GeoDev G, const double* __restrict
     ws[g] = make_double2(wg * sx, wg * sy);
     double rx = sx - t1 + t3 * (p.y - yb), ry = sy - t2 - t3 * (p.x - xb);
     double2 v = make_double2(wg * rx, wg * ry);
-    wrest[g] = v;
-    ws32[g] = make_float2((float)v.x, (float)v.y);
+    const double2 nn = G.nrm[g];
+    sq64[g] = pair_tensor64(nn, v);
+    sq32[g] = pair_tensor32(nn, v);
   }
 }
 
@@ -278,10 +292,10 @@ __device__ __forceinline__ double rcp_variant(double r2) {
 // One CTA's share of the FP64 far field: targets of block bx, tiles of split
 // 'split'.  Shared by k_far64 and the ensemble kernel k_far64_batch.
 template <bool MASK, int NT, int TPT, int RCP>
-__device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __restrict__ ws,
+__device__ __forceinline__ void far64_cta(const GeoDev& G, const double4* __restrict__ sq,
                                           const int4* __restrict__ tiles, const int* __restrict__ split_ptr,
                                           const unsigned* __restrict__ mask, int mw, double2* __restrict__ partial,
-                                          int bx, int split, double4* sg, double2* sw) {
+                                          int bx, int split, double4* sg, double* sw) {
   const int N = G.N;
   const int i0 = bx * (NT * TPT) + threadIdx.x;
   int it[TPT], cv[TPT];
@@ -300,9 +314,10 @@ __device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __rest
     __syncthreads();
     for (int k = threadIdx.x; k < T.y; k += NT) {
       int g = T.x + k;
-      double2 q = G.xy[g], nn = G.nrm[g];
-      sg[k] = make_double4(q.x, q.y, nn.x, nn.y);
-      sw[k] = ws[g];
+      const double2 q = G.xy[g];
+      const double4 S = sq[g];
+      sg[k] = make_double4(q.x, q.y, S.x, S.y);
+      sw[k] = S.z;
     }
     __syncthreads();
     double tx[TPT], ty[TPT];
@@ -310,16 +325,18 @@ __device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __rest
     for (int q = 0; q < TPT; ++q) { tx[q] = 0.0; ty[q] = 0.0; }
 #pragma unroll 2
     for (int j = 0; j < T.y; ++j) {
-      const double4 s = sg[j];
-      const double2 a = sw[j];
+      const double4 s = sg[j];   // x, y, S_xx, 2 S_xy
+      const double syy = sw[j];
 #pragma unroll
       for (int q = 0; q < TPT; ++q) {
-        double rx = px[q] - s.x, ry = py[q] - s.y;
-        double rho2 = fma(rx, rx, ry * ry);
-        double rdn = fma(rx, s.z, ry * s.w);
-        double rds = fma(rx, a.x, ry * a.y);
-        double inv = rcp_variant<RCP>(rho2);
-        double c = rdn * rds * inv * inv;
+        // (r.n)(r.v) = r^T S r = (S_xx r_x + 2 S_xy r_y) r_x + S_yy r_y^2
+        const double rx = px[q] - s.x, ry = py[q] - s.y;
+        const double ry2 = ry * ry;
+        const double rho2 = fma(rx, rx, ry2);
+        const double t = fma(s.w, ry, s.z * rx);
+        const double qq = fma(t, rx, syy * ry2);
+        const double inv = rcp_variant<RCP>(rho2);
+        const double c = qq * inv * inv;
         tx[q] = fma(c, rx, tx[q]);
         ty[q] = fma(c, ry, ty[q]);
       }
@@ -340,12 +357,12 @@ __device__ __forceinline__ void far64_cta(const GeoDev& G, const double2* __rest
 
 template <bool MASK, int NT, int TPT, int RCP>
 __global__ void __launch_bounds__(NT, 512 / NT)
-k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles,
+k_far64(GeoDev G, const double4* __restrict__ sq, const int4* __restrict__ tiles,
         const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
         double2* __restrict__ partial) {
   __shared__ double4 sg[FAR_TS];
-  __shared__ double2 sw[FAR_TS];
-  far64_cta<MASK, NT, TPT, RCP>(G, ws, tiles, split_ptr, mask, mw, partial, blockIdx.x, blockIdx.y, sg, sw);
+  __shared__ double sw[FAR_TS];
+  far64_cta<MASK, NT, TPT, RCP>(G, sq, tiles, split_ptr, mask, mw, partial, blockIdx.x, blockIdx.y, sg, sw);
 }
 
 // ---------------------------------------------------------------------------
@@ -361,12 +378,16 @@ k_far64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ tiles
 // FP64, so r = (c_t - c_s) + (o_t - o_s) is rounded relative to |r|, not to the
 // magnitude of the coordinates.
 //
-// Arithmetic: sm_100's packed FP32 instructions (two lanes per instruction,
-// each lane IEEE round-to-nearest exactly like the scalar instruction) process
-// two targets per instruction against one source, so every pair costs the same
-// rounded operations as the scalar form while the instruction count halves.
-// The source record is duplicated into both lanes when it is staged in shared
-// memory: (-x, -x, -y, -y), (nx, nx, ny, ny), (wx, wx, wy, wy).
+// Arithmetic: the pair term (r.n)(r.v) r / rho^4 is evaluated as
+// (r^T S r) r / rho^4 with the source's symmetric tensor S (pair_tensor32,
+// formed in FP64 by k_prep): t = S_xx r_x + 2 S_xy r_y, q = t r_x + S_yy r_y^2,
+// c = (q / rho^2) / rho^2 — 12 lane operations and one reciprocal per pair.
+// sm_100's packed FP32 instructions (two lanes per instruction, each lane IEEE
+// round-to-nearest exactly like the scalar instruction) process two targets per
+// instruction against one source, so every pair costs the same rounded
+// operations as the scalar form while the instruction count halves.  The
+// source record is duplicated into both lanes when it is staged in shared
+// memory: (-x, -x, -y, -y), (S_xx, S_xx, 2 S_xy, 2 S_xy), (S_yy, S_yy).
 constexpr int F32_TS = 256;
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -407,10 +428,10 @@ constexpr int F32_CHUNK = 16;
 template <bool MASK, int NT, int TPT, int U>
 __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* __restrict__ src,
                                           const float2* __restrict__ tgt, const double2* __restrict__ anchor,
-                                          const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+                                          const double2* __restrict__ tile_c, const float4* __restrict__ sq32,
                                           const int4* __restrict__ tiles, const int* __restrict__ split_ptr,
                                           const unsigned* __restrict__ mask, int mw, double2* __restrict__ partial,
-                                          int bx, int split, float4* s_pos, float4* s_nrm, float4* s_den) {
+                                          int bx, int split, float4* s_pos, float4* s_q1, float2* s_q2) {
   static_assert(TPT % 2 == 0, "targets are processed in lane pairs");
   static_assert(F32_CHUNK % U == 0, "the source-loop unroll divides the chunk");
   constexpr int TP = TPT / 2;
@@ -431,18 +452,18 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
     __syncthreads();
     for (int k = threadIdx.x; k < T.y; k += NT) {
       const float4 a = src[T.x + k];
-      const float2 w = ws32[T.x + k];
+      const float4 q = sq32[T.x + k];
       s_pos[k] = make_float4(-a.x, -a.x, -a.y, -a.y);
-      s_nrm[k] = make_float4(a.z, a.z, a.w, a.w);
-      s_den[k] = make_float4(w.x, w.x, w.y, w.y);
+      s_q1[k] = make_float4(q.x, q.x, q.y, q.y);
+      s_q2[k] = make_float2(q.z, q.z);
     }
     // pad the last chunk with zero-strength sources far from every target
     // (exactly zero terms)
     const int tlen = (T.y + F32_CHUNK - 1) / F32_CHUNK * F32_CHUNK;
     for (int k = T.y + threadIdx.x; k < tlen; k += NT) {
       s_pos[k] = make_float4(-1e4f, -1e4f, -1e4f, -1e4f);
-      s_nrm[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      s_den[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      s_q1[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      s_q2[k] = make_float2(0.f, 0.f);
     }
     __syncthreads();
     const double2 cs = tile_c[ti];
@@ -469,19 +490,22 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
       for (int p = 0; p < TP; ++p) TX[p] = TY[p] = make_float2(0.f, 0.f);
 #pragma unroll U
       for (int j = j0; j < j0 + F32_CHUNK; ++j) {
-        const float4 A = s_pos[j], B = s_nrm[j], C = s_den[j];
+        const float4 A = s_pos[j], B = s_q1[j];
+        const float2 qyy = s_q2[j];
         const float2 msx = make_float2(A.x, A.y), msy = make_float2(A.z, A.w);
-        const float2 nx = make_float2(B.x, B.y), ny = make_float2(B.z, B.w);
-        const float2 wx = make_float2(C.x, C.y), wy = make_float2(C.z, C.w);
+        const float2 qxx = make_float2(B.x, B.y), qxy = make_float2(B.z, B.w);
 #pragma unroll
         for (int p = 0; p < TP; ++p) {
+          // 12 lane operations and one reciprocal per pair:
+          // c = r^T S r / rho^4,  u += c r
           const float2 rx = __fadd2_rn(PX[p], msx);
           const float2 ry = __fadd2_rn(PY[p], msy);
-          const float2 rho2 = __ffma2_rn(rx, rx, __fmul2_rn(ry, ry));
-          const float2 rdn = __ffma2_rn(rx, nx, __fmul2_rn(ry, ny));
-          const float2 rds = __ffma2_rn(rx, wx, __fmul2_rn(ry, wy));
+          const float2 ry2 = __fmul2_rn(ry, ry);
+          const float2 rho2 = __ffma2_rn(rx, rx, ry2);
           const float2 inv = make_float2(rcp_approx(rho2.x), rcp_approx(rho2.y));
-          const float2 c = __fmul2_rn(__fmul2_rn(rdn, rds), __fmul2_rn(inv, inv));
+          const float2 t = __ffma2_rn(qxy, ry, __fmul2_rn(qxx, rx));
+          const float2 q = __ffma2_rn(t, rx, __fmul2_rn(qyy, ry2));
+          const float2 c = __fmul2_rn(__fmul2_rn(q, inv), inv);
           TX[p] = __ffma2_rn(c, rx, TX[p]);
           TY[p] = __ffma2_rn(c, ry, TY[p]);
         }
@@ -511,14 +535,14 @@ __host__ __device__ constexpr int far32_min_blocks(int nt, int tpt) { return (tp
 template <bool MASK, int NT, int TPT, int U>
 __global__ void __launch_bounds__(NT, far32_min_blocks(NT, TPT))
 k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
-        const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
+        const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float4* __restrict__ sq32,
         const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
         double2* __restrict__ partial) {
   __shared__ float4 s_pos[F32_TS];
-  __shared__ float4 s_nrm[F32_TS];
-  __shared__ float4 s_den[F32_TS];
-  far32_cta<MASK, NT, TPT, U>(N, nout, n, src, tgt, anchor, tile_c, ws32, tiles, split_ptr, mask, mw, partial,
-                           blockIdx.x, blockIdx.y, s_pos, s_nrm, s_den);
+  __shared__ float4 s_q1[F32_TS];
+  __shared__ float2 s_q2[F32_TS];
+  far32_cta<MASK, NT, TPT, U>(N, nout, n, src, tgt, anchor, tile_c, sq32, tiles, split_ptr, mask, mw, partial,
+                           blockIdx.x, blockIdx.y, s_pos, s_q1, s_q2);
 }
 
 // ---------------------------------------------------------------------------
@@ -527,7 +551,7 @@ k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __
 // items are numbered job by job (FarJob*.item0) and CTAs stride over them.
 struct FarJob64 {
   GeoDev G;
-  const double2* ws;
+  const double4* sq;
   const int4* tiles;
   const int* split_ptr;
   const unsigned* mask;   // nullptr: no near masking
@@ -543,7 +567,7 @@ struct FarJob32 {
   const float2* tgt;
   const double2* anchor;
   const double2* tile_c;
-  const float2* ws32;
+  const float4* sq32;
   const int4* tiles;
   const int* split_ptr;
   const unsigned* mask;
@@ -568,13 +592,13 @@ template <int NT, int TPT, int RCP>
 __global__ void __launch_bounds__(NT, 512 / NT)
 k_far64_batch(const FarJob64* __restrict__ jobs, int njobs, long long nitems) {
   __shared__ double4 sg[FAR_TS];
-  __shared__ double2 sw[FAR_TS];
+  __shared__ double sw[FAR_TS];
   for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
     const FarJob64 J = jobs[find_job(jobs, njobs, item)];
     const int local = (int)(item - J.item0);
     const int bx = local % J.nbx, q = local / J.nbx;
-    if (J.mask) far64_cta<true, NT, TPT, RCP>(J.G, J.ws, J.tiles, J.split_ptr, J.mask, J.mw, J.partial, bx, q, sg, sw);
-    else far64_cta<false, NT, TPT, RCP>(J.G, J.ws, J.tiles, J.split_ptr, nullptr, 0, J.partial, bx, q, sg, sw);
+    if (J.mask) far64_cta<true, NT, TPT, RCP>(J.G, J.sq, J.tiles, J.split_ptr, J.mask, J.mw, J.partial, bx, q, sg, sw);
+    else far64_cta<false, NT, TPT, RCP>(J.G, J.sq, J.tiles, J.split_ptr, nullptr, 0, J.partial, bx, q, sg, sw);
     __syncthreads();
   }
 }
@@ -583,18 +607,18 @@ template <int NT, int TPT, int U>
 __global__ void __launch_bounds__(NT, far32_min_blocks(NT, TPT))
 k_far32_batch(const FarJob32* __restrict__ jobs, int njobs, long long nitems) {
   __shared__ float4 s_pos[F32_TS];
-  __shared__ float4 s_nrm[F32_TS];
-  __shared__ float4 s_den[F32_TS];
+  __shared__ float4 s_q1[F32_TS];
+  __shared__ float2 s_q2[F32_TS];
   for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
     const FarJob32 J = jobs[find_job(jobs, njobs, item)];
     const int local = (int)(item - J.item0);
     const int bx = local % J.nbx, q = local / J.nbx;
     if (J.mask)
-      far32_cta<true, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.ws32, J.tiles, J.split_ptr,
-                               J.mask, J.mw, J.partial, bx, q, s_pos, s_nrm, s_den);
+      far32_cta<true, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.sq32, J.tiles, J.split_ptr,
+                               J.mask, J.mw, J.partial, bx, q, s_pos, s_q1, s_q2);
     else
-      far32_cta<false, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.ws32, J.tiles, J.split_ptr,
-                                nullptr, 0, J.partial, bx, q, s_pos, s_nrm, s_den);
+      far32_cta<false, NT, TPT, U>(J.N, J.nout, J.n, J.src, J.tgt, J.anchor, J.tile_c, J.sq32, J.tiles, J.split_ptr,
+                                nullptr, 0, J.partial, bx, q, s_pos, s_q1, s_q2);
     __syncthreads();
   }
 }
@@ -685,13 +709,6 @@ k_self64(GeoDev G, const double2* __restrict__ ws, const int4* __restrict__ task
     }
   }
   if (act) out[(size_t)chunk * G.N + i] = make_double2(ax, ay);
-}
-
-__global__ void k_ws32(int N, const double2* __restrict__ ws, float2* __restrict__ out) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= N) return;
-  double2 a = ws[g];
-  out[g] = make_float2((float)a.x, (float)a.y);
 }
 
 // ---------------------------------------------------------------------------

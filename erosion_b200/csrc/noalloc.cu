@@ -200,8 +200,8 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
     double2* cen = cv.take<double2>(std::max(M, 1));
     double* rb = cv.take<double>(std::max(M, 1));
     double2* ws = cv.take<double2>(N);
-    double2* wrest = cv.take<double2>(N);
-    float2* ws32 = cv.take<float2>(N);
+    double4* sq64 = cv.take<double4>(N);
+    float4* sq32 = cv.take<float4>(N);
     double* sigdotn = cv.take<double>(1);
     int4* tiles = cv.take<int4>(ntile);
     int4* tasks = cv.take<int4>(ntask);
@@ -232,10 +232,10 @@ extern "C" int erosion_matvec_noalloc(const erosion_params* p, int64_t npts, int
       k_body_stats<<<M, 256, 0, st>>>(n, nout, xy, sp, cen, rb);
       EB_LAUNCH_CHECK();
     }
-    k_prep<<<M + 1, 256, 0, st>>>(G, d_den, ws, wrest, ws32, d_vel, sigdotn, 0);
+    k_prep<<<M + 1, 256, 0, st>>>(G, d_den, ws, sq64, sq32, d_vel, sigdotn, 0);
     EB_LAUNCH_CHECK();
     k_far64<false, FAR_NT, FAR_TPT, 0><<<dim3((unsigned)TB, (unsigned)nsplit), FAR_NT, 0, st>>>(
-        G, wrest, tiles, split_ptr, nullptr, 0, partial);
+        G, sq64, tiles, split_ptr, nullptr, 0, partial);
     EB_LAUNCH_CHECK();
     k_self64<<<ntask, 256, 0, st>>>(G, ws, tasks, selfsum, n);   // one chunk per body
     EB_LAUNCH_CHECK();

@@ -271,7 +271,7 @@ static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Sha
               "launch_far's FP32 cases");
 
 // One far-field launch of the given kind (0 accurate FP64 and 2 fast FP64 on
-// wrest, 1 FP32 on ws32) and shape over the tile splits sp[0..nsplit], into
+// sq64, 1 FP32 on sq32) and shape over the tile splits sp[0..nsplit], into
 // out[split * N + i].
 static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit, double2* out) {
   const Problem& pr = s.pr;
@@ -284,17 +284,17 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
   case IDX:                                                                                                       \
     if (mk)                                                                                                       \
       k_far32<true, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p, \
-                                               s.ws32.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);           \
+                                               s.sq32.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);           \
     else                                                                                                          \
       k_far32<false, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,           \
-                                                s.tile_c.p, s.ws32.p, s.tiles.p, sp, nullptr, 0, out);    \
+                                                s.tile_c.p, s.sq32.p, s.tiles.p, sp, nullptr, 0, out);    \
     break;
 #define EB_FAR64(IDX, NT, TPT, RCP)                                                                          \
   case IDX:                                                                                                  \
     if (mk)                                                                                                  \
-      k_far64<true, NT, TPT, RCP><<<g, NT, 0, st>>>(G, s.wrest.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);     \
+      k_far64<true, NT, TPT, RCP><<<g, NT, 0, st>>>(G, s.sq64.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);     \
     else                                                                                                     \
-      k_far64<false, NT, TPT, RCP><<<g, NT, 0, st>>>(G, s.wrest.p, s.tiles.p, sp, nullptr, 0, out);          \
+      k_far64<false, NT, TPT, RCP><<<g, NT, 0, st>>>(G, s.sq64.p, s.tiles.p, sp, nullptr, 0, out);          \
     break;
   if (kind == 1) {
     switch (shape) {
@@ -370,8 +370,8 @@ static void plan_far(State& s) {
       best = s.tuned_shape[kind];
     } else if (tune) {
       if (!zeroed) {
-        EB_CK(cudaMemsetAsync(s.ws32.p, 0, sizeof(float2) * pr.N, s.st));
-        EB_CK(cudaMemsetAsync(s.wrest.p, 0, sizeof(double2) * pr.N, s.st));
+        EB_CK(cudaMemsetAsync(s.sq32.p, 0, sizeof(float4) * pr.N, s.st));
+        EB_CK(cudaMemsetAsync(s.sq64.p, 0, sizeof(double4) * pr.N, s.st));
         zeroed = true;
       }
       float bestms = 1e30f;
@@ -438,7 +438,7 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   s.xy.ensure(N); s.nrm.ensure(N); s.dz.ensure(N); s.d1tmp.ensure(N);
   s.sp.ensure(N); s.cur.ensure(N); s.w.ensure(N);
   s.cen.ensure(std::max(pr.M, 1)); s.rb.ensure(std::max(pr.M, 1));
-  s.ws.ensure(N); s.wrest.ensure(N); s.sigdotn.ensure(1);
+  s.ws.ensure(N); s.sq64.ensure(N); s.sigdotn.ensure(1);
   k_wall_nodes<<<nblk(pr.nout, 256), 256, 0, st>>>(pr.nout, pr.P.wall_a, pr.P.wall_b, pr.P.wall_order, s.wx.p, s.wy.p);
   EB_LAUNCH_CHECK();
   k_geom<<<1, 1024, 0, st>>>(s.wx.p, s.wy.p, pr.nout, s.dker_wall.p, 0, 1, s.xy.p, s.nrm.p, s.sp.p, s.cur.p, s.w.p,
@@ -471,7 +471,7 @@ void setup_problem(State& s, const Problem& in, const double* d_xx, const double
   build_near(s, hxy, hsp, hcen, hrb);
   build_tiles(s);
   s.src32.ensure(N);
-  s.ws32.ensure(N);
+  s.sq32.ensure(N);
   s.tgt32.ensure(N);
   s.anchor.ensure(N);
   s.selfsum.ensure((size_t)s.n_self_slots * N);
@@ -639,7 +639,7 @@ void harvest_far_timing(State& s) {
 
 void operator_prep(State& s, const double* d_den, double* d_vel) {
   const Problem& pr = s.pr;
-  k_prep<<<pr.M + 1, 256, 0, s.st>>>(s.geo(), d_den, s.ws.p, s.wrest.p, s.ws32.p, d_vel, s.sigdotn.p,
+  k_prep<<<pr.M + 1, 256, 0, s.st>>>(s.geo(), d_den, s.ws.p, s.sq64.p, s.sq32.p, d_vel, s.sigdotn.p,
                                       pr.P.ibary == 1);
   EB_LAUNCH_CHECK();
 }
@@ -973,7 +973,8 @@ void release_state_buffers(State& s) {
                          &s.d_xx, &s.d_yy, &s.d_den, &s.d_rhs, &s.d_r, &s.d_w, &s.V, &s.Z, &s.part, &s.hdev,
                          &s.ydev, &s.pc_z, &s.pc_u};
   for (auto* b : dbs) b->release();
-  DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.wrest, &s.partial, &s.bd, &s.pair_out};
+  DBuf<double2>* d2s[] = {&s.xy, &s.nrm, &s.dz, &s.cen, &s.d1tmp, &s.ws, &s.partial, &s.bd, &s.pair_out};
+  s.sq64.release();
   for (auto* b : d2s) b->release();
   s.near.src_curve.release(); s.near.pair_tgt.release(); s.near.tptr.release(); s.near.tpairs.release();
   s.near.bd_off.release(); s.near.bd_work.release(); s.near.bary_work.release(); s.near.mask.release();
@@ -982,7 +983,7 @@ void release_state_buffers(State& s) {
   s.zcap = 0;
   s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
   s.pc_valid = false;
-  s.src32.release(); s.ws32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
+  s.src32.release(); s.sq32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
   s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();
   s.split_tune.release(); s.split_ptr64f.release(); s.tune_N = -1;
   for (int k = 0; k < kFarKinds; ++k) s.tuned_shape[k] = -1;

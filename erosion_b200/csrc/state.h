@@ -138,7 +138,8 @@ struct State {
   cudaEvent_t et0 = nullptr, et1 = nullptr;
   // mixed precision: FP32 geometry, strengths, self-curve tasks and sums
   DBuf<float4> src32;
-  DBuf<float2> ws32, tgt32;
+  DBuf<float4> sq32;        // FP32 far-field source tensors (pair_tensor32)
+  DBuf<float2> tgt32;
   DBuf<double2> tile_c, anchor;
   DBuf<int4> self_tasks;
   int n_self_tasks = 0, n_self_slots = 1, n_self_wall = 1, n_self_body = 1;
@@ -161,7 +162,8 @@ struct State {
   int far_kind = 0;   // kind of the far launch bracketed by ef0/ef1: 0 FP64, 1 FP32, 2 fast FP64
 
   // work buffers
-  DBuf<double2> ws, wrest, partial, bd, pair_out;
+  DBuf<double2> ws, partial, bd, pair_out;
+  DBuf<double4> sq64;        // FP64 far-field source tensors (pair_tensor64)
   DBuf<double> sigdotn;
   DBuf<double> d_xx, d_yy, d_den, d_rhs, d_r, d_w;
 
