@@ -74,7 +74,7 @@ TRAFFIC_BYTES_PER_NODE = {"k_far64": 1780224 / 27648, "k_far32": 1737472 / 27648
 # leg of this script measures them on the GPU.  Used only by the reference
 # arm's model for workloads whose CPU solve cannot finish in minutes; on c1
 # the reference arm runs the oracle's own GMRES instead.
-PLAIN_ITERATIONS_PER_STEP = {"c2": 3165, "c3": 12046, "c5": 6000}
+PLAIN_ITERATIONS_PER_STEP = {"c2": 3165, "c3": 12046}
 
 
 def parse(argv=None):
@@ -274,10 +274,10 @@ def run_reference(args, world, rank):
     a model from timed samples at the larger workloads."""
     if rank != 0:
         return
-    if args.workload == "c4":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference arm is defined per geometry (c1-c3, "
-                                                              "c5); the ensemble has no plain iteration count to "
-                                                              "scale the CPU sample by"}))
+    if args.workload != "c1" and args.workload not in PLAIN_ITERATIONS_PER_STEP:
+        print(json.dumps({"impl": "reference", "unavailable": f"no measured plain GMRES iteration count for "
+                                                              f"{args.workload} to scale the CPU operator sample by "
+                                                              f"(the arm is defined for c1, c2 and c3)"}))
         return
     from erosion_b200 import geometry as G
     from oracle import Oracle
