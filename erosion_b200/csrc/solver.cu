@@ -524,8 +524,8 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
   if (have_x) EB_CK(cudaMemcpyAsync(c, d_x, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
   if (have_x && lw_guess_increment(s, d_hist, c)) {
     // the network predicts the bodies' increment only: update the wall
-    // density by Richardson sweeps on the wall rows (wall block ~ -1/2 I)
-    for (int it = 0; it < 3; ++it) {
+    // density by one Richardson sweep on the wall rows (wall block ~ -1/2 I)
+    for (int it = 0; it < 1; ++it) {
       rel_res(c);
       k_wall_richardson<<<nblk(2LL * s.pr.nout, 256), 256, 0, st>>>(s.pr.nout, r, c);
       EB_LAUNCH_CHECK();
