@@ -364,7 +364,10 @@ def run_ensemble(args, world, rank, local, dist):
                            "bodies": [g.M for g in E], "nodes_per_body": [g.n for g in E],
                            "precision": "mixed" if args.precision else "fp64", "precond": args.precond,
                            "step": "one solve of every geometry (wall clock of erosion_solve_batch, host arrays)"},
-                "device_ms_per_step": dev_ms, "rounds": st["rounds"], "iterations": st["iterations"],
+                "device_ms_per_step": dev_ms,
+                "host_time_share": max(0.0, 1.0 - dev_ms / ms),
+                "setup_host_ms": float(np.mean([s["setup_host_ms"] for s in stats])),
+                "rounds": st["rounds"], "iterations": st["iterations"],
                 "graph_captures": st["graph_captures"], "max_true_residual": st["max_true_residual"],
                 "far_pairs_per_s": (st["pairs64_total"] + st["pairs32_total"]) / (dev_ms * 1e-3),
                 "one_by_one": {"ms": seq_ms, "device_ms_in_solves": seq_dev,
