@@ -879,6 +879,133 @@ k_pc_identity_if_bad(int m, const int* __restrict__ bad, float* __restrict__ B) 
   }
 }
 
+// Blocked form of k_gj_inv32: the same in-place Gauss-Jordan inversion with
+// partial pivoting, the pivots taken pb at a time.  A panel of pb columns is
+// loaded into shared memory and eliminated there (pivot search, row scaling
+// and elimination of every other row restricted to the panel); the elementary
+// row operations of the panel compose into L = I + (P - I_panel) E^T, whose
+// panel columns P are exactly what in-place Gauss-Jordan leaves in the panel.
+// The other columns then take the whole panel at once: with W the panel's
+// pivot rows of those columns (after the panel's row swaps),
+//   A[i][j] <- (i a panel pivot row ? 0 : A[i][j]) + sum_k P[i][k] W[k][j],
+// one pass over the matrix per panel instead of one per pivot.  Row swaps are
+// applied to the non-panel columns in global memory; at the end they are
+// undone as column swaps, last first.  Shared memory: m*pb (P) + pb*m (W) +
+// m (pivot column) floats + m ints.  A zero pivot sets bad[matrix].
+__global__ void __launch_bounds__(512)
+k_gj_inv32_blocked(int m, int pb, float* __restrict__ B, int* __restrict__ bad) {
+  extern __shared__ float gjb[];
+  float* P = gjb;                        // m x pb, row i at P[i * pb]
+  float* W = gjb + (size_t)m * pb;       // pb x m
+  float* pcol = W + (size_t)pb * m;      // m
+  int* piv = (int*)(pcol + m);           // m
+  __shared__ float rv[32];
+  __shared__ int ri[32];
+  __shared__ float dsh;
+  float* A = B + (size_t)blockIdx.x * m * m;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k0 = 0; k0 < m; k0 += pb) {
+    const int kb = min(pb, m - k0);
+    for (int e = tid; e < m * kb; e += nt) {
+      const int i = e / kb, k = e - i * kb;
+      P[i * pb + k] = A[(size_t)i * m + k0 + k];
+    }
+    __syncthreads();
+    for (int k = 0; k < kb; ++k) {
+      const int kk = k0 + k;
+      float best = -1.f;
+      int bi = kk;
+      for (int i = kk + tid; i < m; i += nt) {
+        const float a = fabsf(P[i * pb + k]);
+        if (a > best) { best = a; bi = i; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
+      }
+      if ((tid & 31) == 0) { rv[tid >> 5] = best; ri[tid >> 5] = bi; }
+      __syncthreads();
+      if (tid < 32) {
+        best = tid < (nt >> 5) ? rv[tid] : -1.f;
+        bi = tid < (nt >> 5) ? ri[tid] : kk;
+        for (int o = 16; o > 0; o >>= 1) {
+          const float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+          const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (b2 > best || (b2 == best && i2 < bi)) { best = b2; bi = i2; }
+        }
+        if (tid == 0) { piv[kk] = bi; if (!(best > 0.f)) bad[blockIdx.x] = 1; }
+      }
+      __syncthreads();
+      const int p = piv[kk];
+      if (p != kk && tid < kb) {
+        const float t = P[kk * pb + tid];
+        P[kk * pb + tid] = P[p * pb + tid];
+        P[p * pb + tid] = t;
+      }
+      __syncthreads();
+      if (tid == 0) dsh = 1.f / P[kk * pb + k];
+      for (int i = tid; i < m; i += nt) pcol[i] = P[i * pb + k];
+      __syncthreads();
+      const float d = dsh;
+      if (tid < kb) P[kk * pb + tid] = (tid == k) ? d : P[kk * pb + tid] * d;
+      __syncthreads();
+      for (int e = tid; e < m * kb; e += nt) {
+        const int i = e / kb, j = e - i * kb;
+        if (i == kk) continue;
+        const float f = pcol[i];
+        P[i * pb + j] = (j == k) ? -f * d : P[i * pb + j] - f * P[kk * pb + j];
+      }
+      __syncthreads();
+    }
+    // the panel's row swaps, on the other columns
+    for (int k = 0; k < kb; ++k) {
+      const int kk = k0 + k, p = piv[kk];
+      if (p != kk) {
+        for (int j = tid; j < m; j += nt) {
+          if (j >= k0 && j < k0 + kb) continue;
+          const float t = A[(size_t)kk * m + j];
+          A[(size_t)kk * m + j] = A[(size_t)p * m + j];
+          A[(size_t)p * m + j] = t;
+        }
+      }
+      __syncthreads();
+    }
+    for (int e = tid; e < kb * m; e += nt) {
+      const int k = e / m, j = e - k * m;
+      W[e] = (j >= k0 && j < k0 + kb) ? 0.f : A[(size_t)(k0 + k) * m + j];
+    }
+    __syncthreads();
+    for (int i = 0; i < m; ++i) {
+      const bool pivot_row = i >= k0 && i < k0 + kb;
+      const float* Pi = P + i * pb;
+      for (int j = tid; j < m; j += nt) {
+        if (j >= k0 && j < k0 + kb) continue;
+        float acc = pivot_row ? 0.f : A[(size_t)i * m + j];
+        for (int k = 0; k < kb; ++k) acc = fmaf(Pi[k], W[k * m + j], acc);
+        A[(size_t)i * m + j] = acc;
+      }
+    }
+    for (int e = tid; e < m * kb; e += nt) {
+      const int i = e / kb, k = e - i * kb;
+      A[(size_t)i * m + k0 + k] = P[i * pb + k];
+    }
+    __syncthreads();
+  }
+  // undo the row swaps as column swaps, last first
+  for (int k = m - 1; k >= 0; --k) {
+    const int p = piv[k];
+    if (p != k) {
+      for (int i = tid; i < m; i += nt) {
+        const float t = A[(size_t)i * m + k];
+        A[(size_t)i * m + k] = A[(size_t)i * m + p];
+        A[(size_t)i * m + p] = t;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // z_b = B_b^{-1} t_b for every body.  t is gathered from v (the body part of
 // the unknown vector) plus the wall coupling tw (per body node, FP64, already
 // the product A_bw z_wall); z is scattered into the same layout.  CTA = (body,

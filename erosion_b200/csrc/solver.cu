@@ -570,10 +570,24 @@ void setup_preconditioner(State& s) {
   EB_LAUNCH_CHECK();
   int* bad = s.pc_bad.ensure(pr.M);
   EB_CK(cudaMemsetAsync(bad, 0, sizeof(int) * pr.M, s.st));
-  const size_t smem = 3 * (size_t)m * sizeof(float);
-  if (smem > 48 * 1024) EB_CK(cudaFuncSetAttribute(k_gj_inv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
-  EB_LAUNCH_CHECK();
+  // blocked Gauss-Jordan: the widest panel whose shared-memory working set
+  // (2 m pb + m floats, m ints) fits; the unblocked kernel past that
+  int pb = 32;
+  auto gj_smem = [m](int b) { return (2 * (size_t)m * b + m) * sizeof(float) + (size_t)m * sizeof(int); };
+  while (pb > 4 && gj_smem(pb) > 200 * 1024) pb /= 2;
+  if (gj_smem(pb) <= 200 * 1024) {
+    const size_t smem = gj_smem(pb);
+    if (smem > 48 * 1024)
+      EB_CK(cudaFuncSetAttribute(k_gj_inv32_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gj_inv32_blocked<<<pr.M, 512, smem, s.st>>>(m, pb, B, bad);
+    EB_LAUNCH_CHECK();
+  } else {
+    const size_t smem = 3 * (size_t)m * sizeof(float);
+    if (smem > 48 * 1024)
+      EB_CK(cudaFuncSetAttribute(k_gj_inv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
+    EB_LAUNCH_CHECK();
+  }
   // a body whose block had a zero pivot gets the identity (left
   // unpreconditioned); the other bodies keep their inverses
   k_pc_identity_if_bad<<<dim3(pr.M, nblk(m, 8)), 256, 0, s.st>>>(m, bad, B);
