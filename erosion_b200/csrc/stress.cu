@@ -302,15 +302,64 @@ k_bary_sum_near(GeoDev G, const double2* __restrict__ bd_all, const int4* __rest
   }
 }
 
+// Per body: the speed-weighted rigid part of its density, sigma_rigid(x) =
+// (t1, t2) + t3 (-(y - yb), x - xb) with (xb, yb) the speed-weighted centroid
+// (the split k_prep makes for the far field), as rig[5 b + (0..4)] = t1, t2,
+// t3, xb, yb.
+__global__ void __launch_bounds__(256)
+k_stress_rigid(GeoDev G, const double* __restrict__ den, double* __restrict__ rig) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x, start = G.nout + b * G.n;
+  double a0 = 0, a1 = 0, s0 = 0, sxw = 0, syw = 0;
+  for (int j = threadIdx.x; j < G.n; j += blockDim.x) {
+    const int g = start + j;
+    const double sp = G.sp[g];
+    const double2 p = G.xy[g];
+    a0 += den[ix_of(G, g)] * sp;
+    a1 += den[iy_of(G, g)] * sp;
+    s0 += sp;
+    sxw += sp * p.x;
+    syw += sp * p.y;
+  }
+  a0 = block_sum<256>(a0, sh);
+  a1 = block_sum<256>(a1, sh);
+  s0 = block_sum<256>(s0, sh);
+  sxw = block_sum<256>(sxw, sh);
+  syw = block_sum<256>(syw, sh);
+  const double xb = sxw / s0, yb = syw / s0;
+  double r0 = 0, r1 = 0;
+  for (int j = threadIdx.x; j < G.n; j += blockDim.x) {
+    const int g = start + j;
+    const double sp = G.sp[g];
+    const double2 p = G.xy[g];
+    const double fx = -(p.y - yb), fy = p.x - xb;
+    r0 += sp * (fx * den[ix_of(G, g)] + fy * den[iy_of(G, g)]);
+    r1 += sp * (fx * fx + fy * fy);
+  }
+  r0 = block_sum<256>(r0, sh);
+  r1 = block_sum<256>(r1, sh);
+  if (threadIdx.x == 0) {
+    rig[5 * b] = a0 / s0;
+    rig[5 * b + 1] = a1 / s0;
+    rig[5 * b + 2] = r1 > 0 ? r0 / r1 : 0.0;
+    rig[5 * b + 3] = xb;
+    rig[5 * b + 4] = yb;
+  }
+}
+
 // Trapezoid deformation tensor of every other curve except the near ones
 // (mask as k_stress_near_mask), as partial sums over the far-field tile
 // splits: out[(split*3 + q)*nb + i].  The same terms as k_stress_trap, the
 // density scaled by the weight when staged and the reciprocal by
-// rcp_newton.
+// rcp_newton.  A source body's density enters without its rigid part
+// (k_stress_rigid): a rigid-motion density has no exterior double layer, and
+// at these distances the trapezoid rule's value for it is below 1e-16 of its
+// size, while the rigid parts (large for the smallest bodies) would otherwise
+// set the rounding error of the sum.
 __global__ void __launch_bounds__(256)
 k_stress_far(GeoDev G, const double* __restrict__ den, const int4* __restrict__ tiles,
              const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
-             double* __restrict__ out) {
+             const double* __restrict__ rig, double* __restrict__ out) {
   __shared__ double4 sg[FAR_TS];   // x, y, nx, ny
   __shared__ double2 ss[FAR_TS];   // w sigma
   const int nb = G.n * G.M;
@@ -330,7 +379,13 @@ k_stress_far(GeoDev G, const double* __restrict__ den, const int4* __restrict__ 
       const double2 q = G.xy[gs], nn = G.nrm[gs];
       const double wg = G.w[gs];
       sg[k] = make_double4(q.x, q.y, nn.x, nn.y);
-      ss[k] = make_double2(den[ix_of(G, gs)] * wg, den[iy_of(G, gs)] * wg);
+      double sx = den[ix_of(G, gs)], sy = den[iy_of(G, gs)];
+      if (T.z > 0) {
+        const double* R = rig + 5 * (T.z - 1);
+        sx -= R[0] - R[2] * (q.y - R[4]);
+        sy -= R[1] + R[2] * (q.x - R[3]);
+      }
+      ss[k] = make_double2(sx * wg, sy * wg);
     }
     __syncthreads();
     if (T.z == mycurve || ((__ldg(mask + (size_t)ic * mw + (T.z >> 5)) >> (T.z & 31)) & 1u)) continue;
@@ -729,8 +784,11 @@ void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E) {
     EB_LAUNCH_CHECK();
     const int nsplit = s.nsplit;
     part.ensure((size_t)nsplit * 3 * nb);
+    static DBuf<double> rig;
+    k_stress_rigid<<<pr.M, 256, 0, s.st>>>(G, d_den, rig.ensure(5LL * pr.M));
+    EB_LAUNCH_CHECK();
     k_stress_far<<<dim3(nblk(nb, 256), nsplit), 256, 0, s.st>>>(G, d_den, s.tiles.p, s.split_ptr.p, smask.p, mw,
-                                                                 part.p);
+                                                                 rig.p, part.p);
     EB_LAUNCH_CHECK();
     k_stress_final<<<nblk(nb, 256), 256, 0, s.st>>>(G, d_den, pnear.p, 1, part.p, nsplit, 1, eself.p, d_tau, d_E);
     EB_LAUNCH_CHECK();

