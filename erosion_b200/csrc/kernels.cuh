@@ -421,7 +421,10 @@ __device__ __forceinline__ void two_sum_add2(float2& hi, float2& lo, float2 t) {
 // rounding error of the plain FP32 accumulation grows with the chunk length
 // instead of the tile length (measured on solution densities: the operator's
 // FP32 error is ~2.5x smaller with chunks of 16 than with whole 256-node tiles).
-constexpr int F32_CHUNK = 16;
+#ifndef EROSION_F32_CHUNK
+#define EROSION_F32_CHUNK 16
+#endif
+constexpr int F32_CHUNK = EROSION_F32_CHUNK;
 
 // One CTA's share of the FP32 far field (targets of block bx, tiles of split
 // 'split'); shared by k_far32 and the ensemble kernel k_far32_batch.
