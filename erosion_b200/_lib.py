@@ -57,7 +57,7 @@ class ErosionParams(ctypes.Structure):
         ("fast_fp64", c_int32),
         ("precond_refresh", c_int32),
         ("stress_all_bary", c_int32),
-        ("reserved", c_int32 * 1),
+        ("sweep_decades", c_int32),
         ("relax_tol", c_double),
     ]
 

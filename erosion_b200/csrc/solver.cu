@@ -958,11 +958,15 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   long long total = 0;
   double prev_tr = 1e300;
   const bool mixed = s.pr.P.precision != 0;
-  for (int sweep = 0; sweep < 6; ++sweep) {
+  double r_start = x0_zero ? bnrm : device_norm(s, r, N);   // residual the sweep starts from
+  const int sd = mixed ? std::max(0, (int)s.pr.P.sweep_decades) : 0;
+  for (int sweep = 0; sweep < 6 + 2 * sd; ++sweep) {
     long long it = 0;
     double rho = 0;
     const double relax = s.pr.P.relax_tol > 0 ? s.pr.P.relax_tol : tol * kRelaxFactor;
-    int rc = gmres_cycle(s, r, d_x, std::max<long long>(maxl - total, 1), tol * bnrm, mixed ? relax * bnrm : 0.0,
+    // a sweep stops at tol, or sd decades below the residual it started from
+    const double cyc_tol = sd > 0 ? std::max(tol * bnrm, r_start * std::pow(10.0, -sd)) : tol * bnrm;
+    int rc = gmres_cycle(s, r, d_x, std::max<long long>(maxl - total, 1), cyc_tol, mixed ? relax * bnrm : 0.0,
                          &it, &rho);
     total += it;
     s.stats.sweeps = sweep + 1;
@@ -975,6 +979,7 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
     *est = tr;
     if (!std::isfinite(tr)) throw Error(EROSION_BREAKDOWN, "non-finite true residual");
     if (tr <= tol) { *iters = total; return EROSION_OK; }
+    r_start = tr * bnrm;
     // The true residual has a rounding floor ~ eps ||A|| ||x|| / ||b|| that
     // can exceed tol when the densities are large (small bodies: ~1.1e-8 on
     // the 400-body channel, where the FP64 form stops on its estimate with a

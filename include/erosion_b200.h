@@ -124,7 +124,15 @@ typedef struct {
                            trapezoid rule beyond (where the two agree to
                            rounding); 1 evaluates every pair barycentrically, as
                            deformation_on_boundary does                          */
-  int32_t reserved[1];
+  int32_t sweep_decades;/* mixed mode: 0 (default) runs the first refinement sweep
+                           to tol; k > 0 stops every sweep once its estimate has
+                           fallen 10^-k below the residual it started from (or to
+                           tol), and the next sweep restarts from the true FP64
+                           residual.  The error an FP32 operator leaves in a sweep
+                           scales with the residual it starts from, so with
+                           relax_tol >= 1 (FP32 far field from the first
+                           iteration) the sweeps stay accurate while no FP64
+                           far-field sum is needed outside the true residuals      */
   double relax_tol;     /* mixed mode: GMRES switches to the FP32 far field once its
                            residual estimate is below relax_tol (relative);
                            0 selects the library default                           */
