@@ -401,7 +401,9 @@ static void plan_far(State& s) {
     else { s.nsplit64f = ns; upload_splits(s, s.split_ptr64f, ns, 0, s.ntile); }
   }
   // the wall-source FP64 launch of the mixed operator, in the FP64 shape
-  s.nsplitw = far_split_count(pr.N, s.nwall_tiles, shape_targets(0, s.far_shape[0]));
+  // (the fast FP64 kind when allowed: these pairs need ~1e-9, not FP64 rounding)
+  const int wk = pr.P.fast_fp64 ? 2 : 0;
+  s.nsplitw = far_split_count(pr.N, s.nwall_tiles, shape_targets(wk, s.far_shape[wk]));
   upload_splits(s, s.split_ptrw, s.nsplitw, 0, s.nwall_tiles);
   if (tune) { s.tune_N = pr.N; s.tune_ntile = s.ntile; s.tune_masked = masked; }
 }
@@ -701,7 +703,8 @@ void apply_operator(State& s, const double* d_den, double* d_vel, int prec) {
   if (kind == 1) {
     // wall sources in FP64, into the partial slots after the FP32 ones
     EB_CK(cudaEventRecord(s.ew0, st));
-    launch_far(s, 0, s.far_shape[0], s.split_ptrw.p, s.nsplitw, s.partial.p + (size_t)n1 * pr.N);
+    const int wk = pr.P.fast_fp64 ? 2 : 0;
+    launch_far(s, wk, s.far_shape[wk], s.split_ptrw.p, s.nsplitw, s.partial.p + (size_t)n1 * pr.N);
     EB_CK(cudaEventRecord(s.ew1, st));
     s.farw_pending = true;
     s.stats.matvecs_fp32++;
