@@ -107,10 +107,11 @@ typedef struct {
                            erosion_lw_train) and start GMRES from whichever of
                            {learned, supplied density, zero} has the smallest FP64
                            residual                                               */
-  int32_t fast_fp64;    /* mixed mode: 1 (default) applies the fast FP64 operator
-                           (far-field reciprocal to ~1e-12 instead of FP64
-                           rounding) while the residual is above relax_tol, 0 the
-                           accurate one; true residuals always use the accurate  */
+  int32_t fast_fp64;    /* mixed mode: 1 (default) applies the fast FP64 far field
+                           (reciprocal to ~1e-12 instead of FP64 rounding) while the
+                           residual is above relax_tol and to the wall's sources
+                           after, 0 the accurate one; true residuals always use
+                           the accurate one                                       */
   int32_t precond_refresh; /* block preconditioner: 0 or 1 rebuilds the body blocks
                            at every set-up; k > 1 keeps the previous inverses for up
                            to k - 1 further set-ups of the same size (consecutive
