@@ -65,3 +65,21 @@ def test_block_preconditioner_tight_parity(lib, oracle):
     den, nits, st = stokes.solve(g, precond=1, tol=1e-13)
     ref, _, _, _ = oracle.solve(g, tol=1e-13)
     assert np.linalg.norm(den - ref) / np.linalg.norm(ref) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["ref-small", "c1"])
+def test_fp32_from_the_first_iteration_with_decade_sweeps(lib, oracle, name):
+    """relax_tol = 1 (FP32 far field from the first iteration) with refinement
+    sweeps of 3 decades each (sweep_decades = 3): every sweep restarts from the
+    true FP64 residual, the FP64 far field runs only for those residuals, and
+    the answer meets the same tolerance and the same oracle bounds."""
+    g = G.workload(name, seed=2)
+    den, nits, st = stokes.solve(g, precision=1, precond=1, relax_tol=1.0, sweep_decades=3)
+    assert st["true_residual"] <= 1e-8
+    assert st["sweeps"] >= 3
+    assert st["far64f_launches"] == 0 and st["far_launches"] == st["sweeps"]   # the true residuals only
+    ref, _, _, _ = oracle.solve(g, tol=1e-13)
+    assert np.linalg.norm(den - ref) / np.linalg.norm(ref) < 1e-6
+    tau, _ = stokes.shear_stress(g, den)
+    tau_o, _ = oracle.shear_stress(g, ref)
+    assert rel(tau, tau_o) < 1e-7
