@@ -100,9 +100,9 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ensemble", type=int, default=64, help="geometries of the c4 ensemble")
-    ap.add_argument("--c5-steps", type=int, default=40,
+    ap.add_argument("--c5-steps", type=int, default=30,
                     help="c5: target number of steps for 50%% of the body area to erode (sets dt)")
-    ap.add_argument("--c5-max-steps", type=int, default=120, help="c5: cap on the steps of each run")
+    ap.add_argument("--c5-max-steps", type=int, default=60, help="c5: cap on the steps of each run")
     ap.add_argument("--train-steps", type=int, default=15,
                     help="c5: steps of the 400-body run whose first-stage densities train the network")
     return ap.parse_args(argv)
