@@ -530,7 +530,7 @@ void finish_cycle(Member& mb, int rc_cycle, double tol) {
   mb.in_cycle = false;
   least_squares_update(mb);
   if (rc_cycle == EROSION_BREAKDOWN) { mb.status = EROSION_BREAKDOWN; mb.done = true; return; }
-  if (s.pr.P.precision == 0) {
+  if (s.pr.P.precision == 0 && !s.pc_active) {   // unpreconditioned FP64: one cycle, as gmres_solve
     mb.status = rc_cycle;
     mb.true_residual = mb.rho / mb.bnrm;
     mb.done = true;

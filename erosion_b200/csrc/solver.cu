@@ -955,7 +955,7 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   // Arnoldi relation A Z = V H holds only to the rounding of A z, and the
   // preconditioned vectors z carry the bodies' large rigid modes, so the
   // estimate can fall orders of magnitude below the true residual (measured
-  // on the 400-body channel: estimate 1e-12, true residual 6e-6); each sweep
+  // on the 400-body channel: estimate 1e-11, true residual 1.6e-7); each sweep
   // restarts from the true FP64 residual until it meets tol or its rounding
   // floor.
   long long total = 0;

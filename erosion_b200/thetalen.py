@@ -47,6 +47,7 @@ class ParamSet:
     tol: float = 1e-8
     precision: int = 0
     warm_start: int = 0
+    stress_all_bary: int = 0   # 1: every shear-stress pair by the barycentric formulas, as the reference
 
     @property
     def epsilon(self) -> float:
@@ -58,7 +59,8 @@ class ParamSet:
 
     def erosion_params(self) -> _lib.ErosionParams:
         return _lib.default_params(wall=tuple(self.wall), tol=self.tol, maxl=self.maxl, ibary=self.ibary,
-                                   ifmm=self.ifmm, ibc=self.ibc, precision=self.precision)
+                                   ifmm=self.ifmm, ibc=self.ibc, precision=self.precision,
+                                   stress_all_bary=self.stress_all_bary)
 
     def step_params(self):
         sp = StepParams()

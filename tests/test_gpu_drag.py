@@ -1,7 +1,16 @@
 """drag (PostProcess.jl:131-162) through erosion_drag against the oracle's
 restatement (oracle/thetalen_oracle.py: drag), on the same solved density:
-totals, per-node shear stress, smoothed |tau| and pressure to 1e-9, for the
-flow and the rotated flow."""
+totals, per-node shear stress, smoothed |tau| and pressure, for the flow and
+the rotated flow (the geometry turned by 90 degrees inside the same wall, so
+the rotated case needs bodies whose turned positions stay inside it: the
+3-body case below; the library rejects a body outside the wall).
+
+With every shear-stress pair evaluated by the barycentric formulas, as the
+reference does (stress_all_bary = 1), everything agrees to 1e-9.  The
+default evaluation (trapezoid rule beyond 12 node spacings) differs from the
+all-barycentric one by the barycentric formulas' own rounding and
+resolution error, which on the 10-body channel's solved density reaches
+1e-9 of the largest value (measured): 1e-8 there."""
 import numpy as np
 import pytest
 
@@ -11,9 +20,16 @@ from oracle import thetalen_oracle as TO
 pytestmark = pytest.mark.gpu
 
 
-def state_and_density(oracle, name, rotation):
-    g = G.workload(name)
-    params = TL.ParamSet(npts=g.n, nouter=g.nout, wall=g.wall, ibc=g.ibc, fixpdrop=False)
+def geometry(name):
+    if name == "turnable":   # turned by 90 degrees, every body stays inside the wall
+        return G.custom(64, 256, [0.2, 0.15, 0.12], [[-0.4, 0.2], [0.3, -0.3], [0.35, 0.4]])
+    return G.workload(name)
+
+
+def state_and_density(oracle, name, rotation, all_bary=1):
+    g = geometry(name)
+    params = TL.ParamSet(npts=g.n, nouter=g.nout, wall=g.wall, ibc=g.ibc, fixpdrop=False,
+                         stress_all_bary=all_bary)
     thld = TL.circs2thlenden(g.n, g.radii, g.centers[:, 0], g.centers[:, 1])
     bodies = [TO.Body(b.theta.copy(), b.len, b.xsm, b.ysm) for b in thld.thlenvec]
     xs, ys = zip(*[TO.getxy(b) for b in bodies])
@@ -30,16 +46,18 @@ def state_and_density(oracle, name, rotation):
     return g, params, thld, bodies, den
 
 
-@pytest.mark.parametrize("name,rotation", [("ref-small", False), ("ref-small", True), ("c1", False)])
-def test_drag_matches_oracle(lib, oracle, name, rotation):
-    g, params, thld, bodies, den = state_and_density(oracle, name, rotation)
+@pytest.mark.parametrize("name,rotation,all_bary", [("ref-small", False, 1), ("turnable", False, 1),
+                                                    ("turnable", True, 1), ("c1", False, 1), ("c1", False, 0)])
+def test_drag_matches_oracle(lib, oracle, name, rotation, all_bary):
+    g, params, thld, bodies, den = state_and_density(oracle, name, rotation, all_bary)
+    tol = 1e-9 if all_bary else 1e-8
     d = TL.drag(thld, params, rotation=rotation)
     (pdx, pdy, vdx, vdy), tau, atau, press = TO.drag(oracle, bodies, den, g.nout, g.wall, g.ibc, params.sigma,
                                                      rotation=rotation)
     want = np.array([pdx, pdy, vdx, vdy])
     got = np.array([d.pdragx, d.pdragy, d.vdragx, d.vdragy])
-    assert np.abs(got - want).max() / np.abs(want).max() < 1e-9
+    assert np.abs(got - want).max() / np.abs(want).max() < tol
     for a, b in ((d.tau_all, tau), (d.atau_all, atau), (d.press_all, press)):
         assert a.shape == b.shape
-        assert np.abs(a - b).max() / np.abs(b).max() < 1e-9
+        assert np.abs(a - b).max() / np.abs(b).max() < tol
     assert d.umax == 1.0
