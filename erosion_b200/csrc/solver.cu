@@ -968,7 +968,11 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
     double rho = 0;
     const double relax = s.pr.P.relax_tol > 0 ? s.pr.P.relax_tol : tol * kRelaxFactor;
     // a sweep stops at tol, or sd decades below the residual it started from
-    const double cyc_tol = sd > 0 ? std::max(tol * bnrm, r_start * std::pow(10.0, -sd)) : tol * bnrm;
+    // when that point is more than a decade above tol (a sweep that would
+    // stop within a decade of tol runs on to it: another restart would cost
+    // more iterations than it saves)
+    double cyc_tol = tol * bnrm;
+    if (sd > 0 && r_start * std::pow(10.0, -sd) > 10.0 * tol * bnrm) cyc_tol = r_start * std::pow(10.0, -sd);
     int rc = gmres_cycle(s, r, d_x, std::max<long long>(maxl - total, 1), cyc_tol, mixed ? relax * bnrm : 0.0,
                          &it, &rho);
     total += it;

@@ -127,9 +127,10 @@ typedef struct {
                            deformation_on_boundary does                          */
   int32_t sweep_decades;/* mixed mode: 0 (default) runs the first refinement sweep
                            to tol; k > 0 stops every sweep once its estimate has
-                           fallen 10^-k below the residual it started from (or to
-                           tol), and the next sweep restarts from the true FP64
-                           residual.  The error an FP32 operator leaves in a sweep
+                           fallen 10^-k below the residual it started from (a
+                           sweep whose stopping point would lie within a decade
+                           of tol runs to tol), and the next sweep restarts from
+                           the true FP64 residual.  The error an FP32 operator leaves in a sweep
                            scales with the residual it starts from, so with
                            relax_tol >= 1 (FP32 far field from the first
                            iteration) the sweeps stay accurate while no FP64

@@ -6,21 +6,23 @@ takes seconds on the host, and the plain method needs thousands), so the
 chain is:
 
 * the FP64 operator against oracle.matvec on a random density (1e-11);
-* the density reference: the GPU's preconditioned FP64 solve at tol 1e-12.
-  Its densities reach ~6e5 in the rotation modes of the smallest bodies
-  (||x|| ~ 4e7 against ||b|| ~ 35): a rigid-motion density is in the null
-  space of the reference's double-layer operator (-1/2 I + D) and reaches
-  the equations only through the stokeslet/rotlet rows, so two FP64
-  evaluations of A x differ there by their rounding, ~3e-11 of the
-  amplitude (measured with the oracle alone: a rotation density of
-  amplitude 6e5 on one body gives 1.7e-5 on that body's nodes, where the
-  exact value is 0).  The oracle's residual of the reference density is
-  therefore ~6e-6 of ||b|| whoever solved it, and the test ties the
-  reference to the oracle with the rigid parts P x (per body, the
-  least-squares fit by two translations and a rotation) taken out:
-  b - A_oracle (x - P x) - A_gpu (P x) must sit at the FP64 floor (5e-8),
-  and the two operators' values on P x, away from the rows where it is
-  not exactly zero, must both be rounding-sized (2e-10 of max |P x|);
+* the density reference: the GPU's preconditioned FP64 solve at tol 1e-12
+  (its own true residual at the FP64 floor, 5e-8).  Its densities reach
+  ~6e5 in the rotation modes of the smallest bodies and ~7e3 on the wall
+  (||x|| ~ 4e7 against ||b|| ~ 35).  A rigid-motion density is in the null
+  space of a body's double-layer block (-1/2 I + D) and reaches the
+  equations only through the stokeslet/rotlet rows, so FP64 evaluations of
+  A x differ there by rounding proportional to the amplitude (measured with
+  the oracle alone: a rotation density of amplitude 6e5 on one body gives
+  1.7e-5 on that body's nodes, where the exact value is 0).  The oracle's
+  residual of the reference density is ~6e-6 of ||b|| (half of it from the
+  rigid parts' rounding, the rest from the large wall and rigid-free
+  densities), which is the rounding of an operator on this ||x||: the test
+  asserts the normwise backward error ||b - A_oracle x|| / (||A|| ||x|| +
+  ||b||) below 1e-11, the operators' own agreement on a random density, and
+  that both operators' values on the rigid parts P x (per body, the
+  least-squares fit by two translations and a rotation), away from the rows
+  where they are not exactly zero, are rounding-sized (2e-10 of max |P x|);
 * the mixed-precision solve at tol 1e-8 against that reference: density to
   1e-6, the pressure drop between the slices x = -0.9 and x = 0.9 (inside the
   channel; the reference's slices at x = +-2 lie outside this wall) to 1e-6;
@@ -39,6 +41,7 @@ import numpy as np
 import pytest
 
 from erosion_b200 import geometry as G, stokes
+from oracle.rigid import rigid_parts as _rigid_parts
 
 pytestmark = pytest.mark.gpu
 
@@ -86,21 +89,7 @@ def test_fp64_operator_matches_oracle_at_c3(lib, oracle, c3):
 
 
 def rigid_parts(g, den):
-    """Per body, the least-squares fit of its density by the rigid motions
-    (1, 0), (0, 1) and (-(y - yc), x - xc) ((xc, yc) the node mean); zero on the
-    wall and in the stokeslet/rotlet unknowns."""
-    n, M, no = g.n, g.M, g.nout
-    x = np.asarray(g.xx).reshape(M, n)
-    y = np.asarray(g.yy).reshape(M, n)
-    P = np.zeros_like(den)
-    one, zero = np.ones(n), np.zeros(n)
-    for b in range(M):
-        rx, ry = x[b] - x[b].mean(), y[b] - y[b].mean()
-        modes = np.stack([np.r_[one, zero], np.r_[zero, one], np.r_[-ry, rx]], 1)
-        off = 2 * no + 2 * n * b
-        c, *_ = np.linalg.lstsq(modes, den[off:off + 2 * n], rcond=None)
-        P[off:off + 2 * n] = modes @ c
-    return P
+    return _rigid_parts(g.n, g.M, g.nout, g.xx, g.yy, den)
 
 
 def test_reference_density_is_an_oracle_solution(lib, oracle, c3, ref):
@@ -113,14 +102,23 @@ def test_reference_density_is_an_oracle_solution(lib, oracle, c3, ref):
     a_free = oracle.matvec(c3, den - P, mode=1)
     a_rig_o = oracle.matvec(c3, P, mode=1)
     a_rig_g = stokes.matvec(c3, P, precision=0)
-    r_oracle = np.linalg.norm(b - a_free - a_rig_o) / nb
+    r = b - a_free - a_rig_o
+    r_oracle = np.linalg.norm(r) / nb
     r_hybrid = np.linalg.norm(b - a_free - a_rig_g) / nb
+    # normwise backward error ||b - A x|| / (||A|| ||x|| + ||b||) with respect
+    # to the oracle's operator, ||A|| bounded below by ||A z|| / ||z|| on a
+    # random z: the reference density solves a problem within this relative
+    # distance of the oracle's
+    z = np.random.default_rng(8).standard_normal(c3.ntot)
+    norm_a = np.linalg.norm(stokes.matvec(c3, z, precision=0)) / np.linalg.norm(z)
+    eta = np.linalg.norm(r) / (norm_a * np.linalg.norm(den) + nb)
     rows = 2 * c3.nout + 2 * c3.n * c3.M   # A (P x) is exactly zero above the stokeslet/rotlet rows
     floor_o = np.abs(a_rig_o[:rows]).max() / np.abs(P).max()
     floor_g = np.abs(a_rig_g[:rows]).max() / np.abs(P).max()
-    print(f"oracle residual {r_oracle:.2e}; with the library's rigid parts {r_hybrid:.2e}; "
+    print(f"oracle residual {r_oracle:.2e} (with the library's values on P x {r_hybrid:.2e}); "
+          f"backward error {eta:.2e} (||A|| >= {norm_a:.3g}, ||x|| = {np.linalg.norm(den):.3g}); "
           f"rounding on P x: oracle {floor_o:.2e}, library {floor_g:.2e} of max |P x|")
-    assert r_hybrid < 5e-8, r_hybrid
+    assert eta < 1e-11, eta
     assert floor_o < 2e-10 and floor_g < 2e-10
     # the stokeslet/rotlet rows of A (P x) are moments of P x: both evaluate them alike
     assert np.abs(a_rig_o[rows:] - a_rig_g[rows:]).max() < 1e-10 * np.abs(a_rig_o[rows:]).max()
