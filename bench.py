@@ -67,11 +67,15 @@ METRIC = "erosion steps/s at 1e-8 residual"
 
 # DRAM bytes per node and far-field launch (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by the node count N) from the ncu
-# captures of the far-field kernels on the 100-body channel (N = 27,648):
-# both kernels read each source and target record once, so a launch moves
-# N x ~64 B at every size.
-TRAFFIC_BYTES_PER_NODE = {"k_far64": 1780224 / 27648, "k_far32": 1737472 / 27648,
-                          "k_far64_fast": 1780224 / 27648, "k_far64_wall_sources": 1780224 / 27648}
+# captures of k_far32 and the fast k_far64 on the 400-body channel (N =
+# 106,496; one operator application with pinned launch shapes).  A launch
+# reads each source and target record once (N x 64 B) and each target's row
+# of the near mask once (N x 4 B per 32 curves: 52 B at 401 curves).  The
+# accurate k_far64 and the wall-source launch read the same records as the
+# fast k_far64 and carry its figure.
+TRAFFIC_BYTES_PER_NODE = {"k_far32": (11398144 + 16384) / 106496, "k_far64_fast": 10671360 / 106496,
+                          "k_far64": 10671360 / 106496, "k_far64_wall_sources": 10671360 / 106496}
+
 
 # Plain FP64 GMRES iterations per erosion step (unpreconditioned, zero initial
 # guess: the reference's algorithm) on the seeded workloads, as the plain_fp64
@@ -557,10 +561,13 @@ class Stepper:
                 arrs[2][:M].cpu().numpy().copy(), arrs[3][:M].cpu().numpy().copy())
 
 
-def kernel_roofline(s0, s1, N, peak64, peak32, ms_timed):
+def kernel_roofline(s0, s1, N, curves, peak64, peak32, ms_timed):
     """Per far-field kernel: launches, time, pairs per launch, achieved
     TFLOP/s (20 flops per pair), fraction of the measured FMA peak of its pipe
-    and the DRAM bytes per launch (ncu figure per node x N)."""
+    and the DRAM bytes per launch (ncu figure per node x N) beside the
+    algorithmic bytes (64 B per node record plus the node's near-mask row,
+    4 B per 32 curves)."""
+    algorithmic = N * (64 + 4 * ((curves + 31) // 32))
     kernels = {}
     spec = (("k_far64", "ms_far", "far_launches", "far64_pairs", peak64),
             ("k_far64_fast", "ms_far64f", "far64f_launches", "far64_pairs", peak64),
@@ -577,7 +584,7 @@ def kernel_roofline(s0, s1, N, peak64, peak32, ms_timed):
                          "achieved_tflops": a, "peak_tflops": peak, "frac": a / peak,
                          "share_of_timed": ms / ms_timed,
                          "traffic_bytes_per_launch": TRAFFIC_BYTES_PER_NODE[name] * N,
-                         "algorithmic_bytes_per_launch": 64 * N}
+                         "algorithmic_bytes_per_launch": algorithmic}
     return kernels
 
 
@@ -607,6 +614,8 @@ def run_steps(args, world, rank, local, dist):
     shapes = _lib.far_shapes()
     L.erosion_set_far_shape(0, shapes["fp64"]["index"])
     L.erosion_set_far_shape(1, shapes["fp32"]["index"])
+    if "fp64_fast" in shapes:
+        L.erosion_set_far_shape(2, shapes["fp64_fast"]["index"])
     S.snapshot()
     M0 = S.M
     torch.cuda.synchronize()
@@ -642,7 +651,7 @@ def run_steps(args, world, rank, local, dist):
     peak32_scalar = L.erosion_peak_tflops(1)
     peak32_packed = L.erosion_peak_tflops(2)
     peak32 = max(peak32_scalar, peak32_packed)
-    kernels = kernel_roofline(s0, s1, N, peak64, peak32, ms)
+    kernels = kernel_roofline(s0, s1, N, M0 + 1, peak64, peak32, ms)
     dom = max(kernels, key=lambda k: kernels[k]["ms_total"]) if kernels else None
     roofline = {"bound": ("fp32" if dom == "k_far32" else "fp64") if dom else None,
                 "achieved": kernels[dom]["achieved_tflops"] if dom else None,
@@ -656,8 +665,8 @@ def run_steps(args, world, rank, local, dist):
                                "wall-source pairs",
                 "peak_source": "of measured: FMA loop on this GPU (erosion_peak_tflops), vector pipe; FP32 = max of "
                                "scalar and packed two-lane FMA",
-                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch of the ncu capture on "
-                                  "the 100-body channel, per node, times N",
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch of the ncu captures of "
+                                  "k_far32 and the fast k_far64 on the 400-body channel, per node, times N",
                 "peaks_measured_tflops": {"fp64": peak64, "fp32_scalar": peak32_scalar,
                                           "fp32_packed": peak32_packed},
                 "launch_shapes": shapes, "kernels": kernels}

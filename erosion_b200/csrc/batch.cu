@@ -44,6 +44,7 @@ struct Member {
   int nb = 1, Rrows = 1;   // dot-product blocks and rows per block
   // host cycle state
   double bnrm = 0, r0nrm = 0, rho = 0, prev_tr = 1e300, abs_tol = 0, relax_abs = 0;
+  double cyc_abs = 0;   // the current cycle's stopping point (tol, or sweep_decades below its start)
   long long kcyc = 0, total = 0, maxl = 0;
   int sweep = 0, prec = 0, status = EROSION_OK;
   bool in_cycle = false, done = false;
@@ -509,6 +510,11 @@ bool start_cycle(Member& mb) {
   mb.rho = mb.r0nrm;
   mb.kcyc = 0;
   if (mb.r0nrm <= mb.abs_tol) return false;
+  // as gmres_solve: a mixed-precision cycle stops sweep_decades below its
+  // start unless that point lies within a decade of tol
+  const int sd = s.pr.P.precision != 0 ? std::max(0, (int)s.pr.P.sweep_decades) : 0;
+  mb.cyc_abs = mb.abs_tol;
+  if (sd > 0 && mb.r0nrm * std::pow(10.0, -sd) > 10.0 * mb.abs_tol) mb.cyc_abs = mb.r0nrm * std::pow(10.0, -sd);
   ensure_capacity(mb);
   k_copy<<<nblk(N, 256), 256, 0, st>>>(mb.r.p, s.V.p, N);
   EB_LAUNCH_CHECK();
@@ -546,7 +552,8 @@ void finish_cycle(Member& mb, int rc_cycle, double tol) {
   const bool floor = mb.sweep > 1 && (tr <= 2.0 * tol || tr > 0.5 * mb.prev_tr);
   if (tr <= tol || floor) { mb.status = EROSION_OK; mb.done = true; return; }
   mb.prev_tr = tr;
-  if (mb.total >= mb.maxl || mb.sweep >= 6) { mb.status = EROSION_MAXITER; mb.done = true; return; }
+  const int sd = std::max(0, (int)s.pr.P.sweep_decades);
+  if (mb.total >= mb.maxl || mb.sweep >= 6 + 2 * sd) { mb.status = EROSION_MAXITER; mb.done = true; return; }
   if (!start_cycle(mb)) finish_cycle(mb, EROSION_OK, tol);
 }
 
@@ -672,6 +679,14 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
         apply_operator(s, mb.x.p, mb.r.p, 0);
         k_bminus<<<nblk(mb.ntot, 256), 256, 0, s.st>>>(mb.b.p, mb.r.p, mb.ntot);
         EB_LAUNCH_CHECK();
+        // as gmres_solve: in the refinement forms a guess no better than zero
+        // is replaced by zero
+        const bool refine = P.precision != 0 || s.pc_active;
+        if (refine && !(device_norm(s, mb.r.p, mb.ntot) < mb.bnrm)) {
+          EB_CK(cudaMemsetAsync(mb.x.p, 0, (size_t)mb.ntot * sizeof(double), s.st));
+          k_copy<<<nblk(mb.ntot, 256), 256, 0, s.st>>>(mb.b.p, mb.r.p, mb.ntot);
+          EB_LAUNCH_CHECK();
+        }
       }
       if (!start_cycle(mb)) finish_cycle(mb, EROSION_OK, P.tol);
       EB_CK(cudaStreamSynchronize(s.st));
@@ -712,7 +727,7 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
         Member& mb = B.m[g];
         key[g] = -1;
         if (mb.done || !mb.in_cycle) continue;
-        mb.prec = (mb.relax_abs > 0.0 && mb.rho < mb.relax_abs) ? 1 : 0;
+        mb.prec = (mb.relax_abs > 0.0 && mb.rho <= mb.relax_abs) ? 1 : 0;
         key[g] = mb.prec;
         if (ensure_capacity(mb) || !mb.pre) capture_member(B, mb, g);
         any = true;
@@ -742,7 +757,7 @@ int erosion_solve_batch(const erosion_params* p, int32_t nbatch, const int64_t* 
         if (flag == 3) throw Error(EROSION_BREAKDOWN, "non-finite value in the Arnoldi process (ensemble)");
         if (flag == 2) { finish_cycle(mb, EROSION_BREAKDOWN, P.tol); continue; }
         mb.rho = rho;
-        if (rho <= mb.abs_tol) finish_cycle(mb, EROSION_OK, P.tol);
+        if (rho <= mb.cyc_abs) finish_cycle(mb, EROSION_OK, P.tol);
         else if (mb.kcyc >= mb.maxl || mb.total >= mb.maxl)
           finish_cycle(mb, rho < mb.r0nrm ? EROSION_MAXITER : EROSION_BREAKDOWN, P.tol);
       }

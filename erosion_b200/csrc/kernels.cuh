@@ -366,11 +366,12 @@ k_far64(GeoDev G, const double4* __restrict__ sq, const int4* __restrict__ tiles
 }
 
 // ---------------------------------------------------------------------------
-// Far field, FP32 with compensated accumulation (the mixed-precision operator).
-// Same sum as k_far64 but over pairs of DIFFERENT curves only (a target's own
-// curve is evaluated in FP64 by k_self64) and without the near-masked pairs.
-// Each tile is summed in FP32 and folded into a two-sum (Knuth) accumulator
-// (hi, lo), so the rounding error grows with the tile length, not with N.
+// Far field, FP32 pair terms with FP64 accumulation (the mixed-precision
+// operator).  Same sum as k_far64 but over pairs of DIFFERENT curves only (a
+// target's own curve is evaluated in FP64 by k_self64) and without the
+// near-masked pairs.  Chunks of F32_CHUNK sources are summed in FP32 and each
+// chunk sum is added to an FP64 accumulator, so the rounding error of the
+// accumulation grows with the chunk length, not with N.
 //
 // Coordinates: every node is stored as an FP32 offset from the FP64 centre of
 // its own tile (tiles never cross a curve and are at most one body or 32 wall
@@ -404,23 +405,14 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float t) {
   lo += e;
 }
 
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
-
-// two_sum_add on two lanes at once (two targets), each lane exactly the
-// scalar form.
-__device__ __forceinline__ void two_sum_add2(float2& hi, float2& lo, float2 t) {
-  const float2 s = __fadd2_rn(hi, t);
-  const float2 bp = __fadd2_rn(s, neg2(hi));
-  const float2 e = __fadd2_rn(__fadd2_rn(hi, neg2(__fadd2_rn(s, neg2(bp)))), __fadd2_rn(t, neg2(bp)));
-  hi = s;
-  lo = __fadd2_rn(lo, e);
-}
-
 // Sources per FP32 partial sum of k_far32: the running FP32 sum of a target is
-// folded into its two-sum accumulator after every F32_CHUNK sources, so the
-// rounding error of the plain FP32 accumulation grows with the chunk length
-// instead of the tile length (measured on solution densities: the operator's
-// FP32 error is ~2.5x smaller with chunks of 16 than with whole 256-node tiles).
+// added to its FP64 accumulator after every F32_CHUNK sources, so the rounding
+// error of the plain FP32 accumulation grows with the chunk length instead of
+// the tile length (measured on solution densities: the operator's FP32 error
+// is ~2.5x smaller with chunks of 16 than with whole 256-node tiles; an
+// emulation of the kernel's arithmetic puts 85% of the remaining error in the
+// pair terms themselves).  The FP64 additions run on the FP64 pipe, idle in
+// this kernel, instead of a two-sum on the FP32 pipe that bounds it.
 #ifndef EROSION_F32_CHUNK
 #define EROSION_F32_CHUNK 16
 #endif
@@ -440,7 +432,7 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
   constexpr int TP = TPT / 2;
   const int i0 = bx * (NT * TPT) + threadIdx.x;
   int it[TPT], cv[TPT];
-  float2 HX[TP], LX[TP], HY[TP], LY[TP];   // two-sum accumulators, lanes = targets 2p, 2p+1
+  double AX[TPT], AY[TPT];   // FP64 accumulators of the chunk sums
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
     int i = i0 + q * NT;
@@ -448,7 +440,7 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
     cv[q] = it[q] < nout ? 0 : 1 + (it[q] - nout) / n;
   }
 #pragma unroll
-  for (int p = 0; p < TP; ++p) HX[p] = LX[p] = HY[p] = LY[p] = make_float2(0.f, 0.f);
+  for (int q = 0; q < TPT; ++q) AX[q] = AY[q] = 0.0;
   const int tb = split_ptr[split], te = split_ptr[split + 1];
   for (int ti = tb; ti < te; ++ti) {
     const int4 T = tiles[ti];
@@ -515,18 +507,15 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
       }
 #pragma unroll
       for (int p = 0; p < TP; ++p) {   // a select, not a product: an own-curve tile holds inf/NaN terms
-        two_sum_add2(HX[p], LX[p], make_float2(U0[p] ? TX[p].x : 0.f, U1[p] ? TX[p].y : 0.f));
-        two_sum_add2(HY[p], LY[p], make_float2(U0[p] ? TY[p].x : 0.f, U1[p] ? TY[p].y : 0.f));
+        if (U0[p]) { AX[2 * p] += (double)TX[p].x; AY[2 * p] += (double)TY[p].x; }
+        if (U1[p]) { AX[2 * p + 1] += (double)TX[p].y; AY[2 * p + 1] += (double)TY[p].y; }
       }
     }
   }
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
     int i = i0 + q * NT;
-    const int p = q >> 1;
-    const float hx = (q & 1) ? HX[p].y : HX[p].x, lx = (q & 1) ? LX[p].y : LX[p].x;
-    const float hy = (q & 1) ? HY[p].y : HY[p].x, ly = (q & 1) ? LY[p].y : LY[p].x;
-    if (i < N) partial[(size_t)split * N + i] = make_double2((double)hx + (double)lx, (double)hy + (double)ly);
+    if (i < N) partial[(size_t)split * N + i] = make_double2(AX[q], AY[q]);
   }
 }
 

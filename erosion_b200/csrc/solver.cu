@@ -183,12 +183,27 @@ static void build_near(State& s, const std::vector<double2>& hxy, const std::vec
   EB_CK(cudaStreamSynchronize(st));   // host vectors go out of scope
 }
 
-// Split-K of the far-field sums: enough (target block, tile range) CTAs for
-// about 8 per SM; contiguous tile ranges of equal count.
-static int far_split_count(int N, int ntile, int targets_per_cta) {
-  int TB = (int)nblk(N, targets_per_cta);
-  int want = (int)std::ceil(8.0 * g_num_sms / TB);
-  return std::max(1, std::min(want, ntile));
+// Split-K of the far-field sums: about 8 (target block, tile range) CTAs per
+// SM, contiguous tile ranges of equal count.  With the kernel's resident CTAs
+// per SM known (resident > 0), the count is chosen within [want/2, 2 want]
+// so that the CTAs fill whole waves: W = CTAs / (SMs x resident) waves leave
+// the SMs partly idle during the last ceil(W) - W of a wave, so the count
+// with the largest W / ceil(W) wins (the smaller count within 0.5%).  At 400
+// bodies the FP32 kernel (104 target blocks, 2 resident CTAs) goes from 12
+// splits (4.2 waves) to 17 (5.97 waves).
+static int far_split_count(int N, int ntile, int targets_per_cta, int resident = 0) {
+  const int TB = (int)nblk(N, targets_per_cta);
+  const int want = std::max(1, std::min((int)std::ceil(8.0 * g_num_sms / TB), ntile));
+  if (resident <= 0) return want;
+  const double conc = (double)g_num_sms * resident;
+  int best = want;
+  double beste = -1.0;
+  for (int ns = std::max(1, want / 2); ns <= std::min(ntile, 2 * want); ++ns) {
+    const double w = (double)TB * ns / conc;
+    const double e = w / std::ceil(w);
+    if (e > beste + 0.005) { beste = e; best = ns; }
+  }
+  return best;
 }
 
 // Tile ranges [t0 + q (t1-t0)/ns, ...) of equal count over tiles [t0, t1).
@@ -326,6 +341,39 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
   EB_LAUNCH_CHECK();
 }
 
+// Resident CTAs per SM of one far-field kernel instance (the occupancy the
+// split count is sized for); 0 when the runtime cannot tell.
+static int far_resident(int kind, int shape, bool masked) {
+  const void* fn = nullptr;
+  int nt = 0;
+#define EB_R32(IDX, NT, TPT, U)                                                                          \
+  case IDX:                                                                                             \
+    fn = masked ? (const void*)k_far32<true, NT, TPT, U> : (const void*)k_far32<false, NT, TPT, U>;     \
+    nt = NT;                                                                                            \
+    break;
+#define EB_R64(IDX, NT, TPT, RCP)                                                                        \
+  case IDX:                                                                                             \
+    fn = masked ? (const void*)k_far64<true, NT, TPT, RCP> : (const void*)k_far64<false, NT, TPT, RCP>; \
+    nt = NT;                                                                                            \
+    break;
+  if (kind == 1) {
+    switch (shape) { EB_R32(0, 256, 4, 2) EB_R32(1, 256, 4, 4) EB_R32(2, 256, 2, 2) EB_R32(3, 256, 2, 4) default: break; }
+  } else if (kind == 0) {
+    switch (shape) { EB_R64(0, 256, 2, 1) EB_R64(1, 128, 4, 1) EB_R64(2, 256, 2, 3) EB_R64(3, 128, 4, 3) default: break; }
+  } else {
+    switch (shape) { EB_R64(0, 256, 2, 2) EB_R64(1, 128, 4, 2) EB_R64(2, 256, 2, 4) EB_R64(3, 128, 4, 4) default: break; }
+  }
+#undef EB_R32
+#undef EB_R64
+  if (!fn) return 0;
+  int r = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fn, nt, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return r;
+}
+
 // Problems below this many node pairs keep the first shape of each list (a
 // launch is a few microseconds; timing would cost more than it saves).
 constexpr double kTuneMinPairs = 2e8;
@@ -344,18 +392,19 @@ static void plan_far(State& s) {
   // always run in FP64 (their densities carry fields that cancel against the
   // bodies' to a few parts in 1e4, beyond FP32's reach)
   const int t32 = s.nwall_tiles, n32 = s.ntile - s.nwall_tiles;
+  const int masked = s.near.npairs > 0;
   int maxs = s.nsplit, max32 = 0, maxw = 0;
   for (int kind = 0; kind < kFarKinds; ++kind)
     for (int sh = 0; sh < far_num_shapes(kind); ++sh) {
+      const int res = far_resident(kind, sh, masked);
       if (kind == 1) {
-        if (n32 > 0) max32 = std::max(max32, far_split_count(pr.N, n32, shape_targets(1, sh)));
+        if (n32 > 0) max32 = std::max(max32, far_split_count(pr.N, n32, shape_targets(1, sh), res));
       } else {
-        maxs = std::max(maxs, far_split_count(pr.N, s.ntile, shape_targets(kind, sh)));
-        maxw = std::max(maxw, far_split_count(pr.N, s.nwall_tiles, shape_targets(kind, sh)));
+        maxs = std::max(maxs, far_split_count(pr.N, s.ntile, shape_targets(kind, sh), res));
+        maxw = std::max(maxw, far_split_count(pr.N, s.nwall_tiles, shape_targets(kind, sh), res));
       }
     }
   s.partial.ensure((size_t)std::max(maxs, max32 + maxw) * pr.N);
-  const int masked = s.near.npairs > 0;
   const bool tune = (double)pr.N * (double)pr.N >= kTuneMinPairs;
   const bool cached = s.tune_N == pr.N && s.tune_ntile == s.ntile && s.tune_masked == masked;
   bool zeroed = false;
@@ -376,7 +425,7 @@ static void plan_far(State& s) {
       }
       float bestms = 1e30f;
       for (int sh = 0; sh < nsh; ++sh) {
-        const int ns = far_split_count(pr.N, tcount, shape_targets(kind, sh));
+        const int ns = far_split_count(pr.N, tcount, shape_targets(kind, sh), far_resident(kind, sh, masked));
         upload_splits(s, s.split_tune, ns, tb, tb + tcount);
         launch_far(s, kind, sh, s.split_tune.p, ns, s.partial.p);
         float ms = 1e30f;
@@ -395,7 +444,7 @@ static void plan_far(State& s) {
       s.tuned_shape[kind] = best;
     }
     s.far_shape[kind] = best;
-    const int ns = far_split_count(pr.N, tcount, shape_targets(kind, best));
+    const int ns = far_split_count(pr.N, tcount, shape_targets(kind, best), far_resident(kind, best, masked));
     if (kind == 1) { s.nsplit32 = ns; upload_splits(s, s.split_ptr32, ns, tb, tb + tcount); }
     else if (kind == 0) { s.nsplit64t = ns; upload_splits(s, s.split_ptr64t, ns, 0, s.ntile); }
     else { s.nsplit64f = ns; upload_splits(s, s.split_ptr64f, ns, 0, s.ntile); }
@@ -403,7 +452,8 @@ static void plan_far(State& s) {
   // the wall-source FP64 launch of the mixed operator, in the FP64 shape
   // (the fast FP64 kind when allowed: these pairs need ~1e-9, not FP64 rounding)
   const int wk = pr.P.fast_fp64 ? 2 : 0;
-  s.nsplitw = far_split_count(pr.N, s.nwall_tiles, shape_targets(wk, s.far_shape[wk]));
+  s.nsplitw = far_split_count(pr.N, s.nwall_tiles, shape_targets(wk, s.far_shape[wk]),
+                              far_resident(wk, s.far_shape[wk], masked));
   upload_splits(s, s.split_ptrw, s.nsplitw, 0, s.nwall_tiles);
   if (tune) { s.tune_N = pr.N; s.tune_ntile = s.ntile; s.tune_masked = masked; }
 }
@@ -776,7 +826,7 @@ static double* pinned(State& s, size_t n) {
 // The Arnoldi step is classical Gram-Schmidt applied twice (two passes of
 // tall-skinny products instead of DORTH's k sequential dot/axpy pairs).
 // d_r holds the initial residual on entry.  Operator precision: FP64, or, when
-// relax_abs > 0, FP32 far field once rho < relax_abs (inexact Krylov: the
+// relax_abs > 0, FP32 far field once rho <= relax_abs (inexact Krylov: the
 // operator error tolerated grows as the residual shrinks).
 static int gmres_cycle(State& s, double* d_r, double* d_x, long long maxl_in, double abs_tol, double relax_abs,
                        long long* iters, double* rho_out) {
@@ -818,7 +868,7 @@ static int gmres_cycle(State& s, double* d_r, double* d_x, long long maxl_in, do
     double* vnew = V + ll * ldv;
     // mixed precision: the fast FP64 operator while the residual is large,
     // the FP32 far field once it is below relax_abs
-    const int prec = relax_abs > 0.0 ? (rho < relax_abs ? 1 : (s.pr.P.fast_fp64 ? 2 : 0)) : 0;
+    const int prec = relax_abs > 0.0 ? (rho <= relax_abs ? 1 : (s.pr.P.fast_fp64 ? 2 : 0)) : 0;
     if (s.pc_active) {
       // flexible GMRES: keep z_k = P^{-1} v_k so that x = x0 + Z y is exactly
       // consistent with the Arnoldi relation A Z = V H whatever the
@@ -908,12 +958,13 @@ static int gmres_cycle(State& s, double* d_r, double* d_x, long long maxl_in, do
   return iflag == 1 ? EROSION_MAXITER : EROSION_OK;
 }
 
-// Default switch point of the mixed-precision operator: FP32 far field once
-// the GMRES residual estimate is below kRelaxFactor * tol (1e-3 at tol 1e-8).
-// Earlier switching leaves a larger gap between the estimated and the true
-// residual, paid for by FP64 refinement restarts (400-body workload with the
-// block preconditioner: switch at 1e-1 -> 1173 iterations, 1e-3 -> 780,
-// 1e-6 -> 820 with fewer FP32 matvecs).
+// Switch point of the mixed-precision operator when relax_tol is 0: FP32 far
+// field once the GMRES residual estimate is below kRelaxFactor * tol (1e-3 at
+// tol 1e-8).  erosion_default_params sets relax_tol = 1 with sweep_decades = 5
+// instead: on the 400-body channel (block preconditioner, tol 1e-8, cold
+// start) that solve takes 776 iterations in 5.28 s, all but 3 far-field sums
+// in FP32, against 611 iterations in 6.09 s with 46% of them in FP64 at
+// relax_tol = 1e-2, and 601 at 1e-3.
 static const double kRelaxFactor = 1e5;
 
 int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long long maxl, double tol,
@@ -962,6 +1013,17 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   double prev_tr = 1e300;
   const bool mixed = s.pr.P.precision != 0;
   double r_start = x0_zero ? bnrm : device_norm(s, r, N);   // residual the sweep starts from
+  if (!x0_zero && !(r_start < bnrm)) {
+    // An initial guess no better than zero (a previous step's density on a
+    // moved geometry: the large rigid-mode parts of the small bodies no
+    // longer match) would cost iterations just to get back to ||b||; start
+    // from zero instead.
+    s.stats.guess_residual[1] = r_start / bnrm;
+    EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
+    residual(true);
+    r_start = bnrm;
+    s.stats.guess_used = 0;
+  }
   const int sd = mixed ? std::max(0, (int)s.pr.P.sweep_decades) : 0;
   for (int sweep = 0; sweep < 6 + 2 * sd; ++sweep) {
     long long it = 0;
@@ -1130,6 +1192,8 @@ void erosion_default_params(erosion_params* p) {
   p->rhs_mode = 0;
   p->true_residual = 0;
   p->fast_fp64 = 1;
+  p->sweep_decades = 5;
+  p->relax_tol = 1.0;
 }
 
 int erosion_last_status(void) { return t_status; }

@@ -409,12 +409,14 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   build_rhs(s, rhs);
   const bool zero = choose_initial_guess(s, rhs, den, have_prev, sp.warm_start == 2,
                                          T.hist_valid[k] ? T.hist[k].p : nullptr);
-  T.stats.guess_used[k] = s.stats.guess_used;
-  T.stats.guess_residual[k] = s.stats.guess_used >= 0 ? s.stats.guess_residual[s.stats.guess_used] : -1;
   long long it = 0;
   double est = 0;
   const long long mv0 = s.stats.matvecs, mv32 = s.stats.matvecs_fp32;
   int rc = gmres_solve(s, rhs, den, zero, s.pr.P.maxl, s.pr.P.tol, &it, &est);
+  // the solve may have replaced a guess no better than zero by zero
+  T.stats.guess_used[k] = s.stats.guess_used;
+  T.stats.guess_residual[k] = s.stats.guess_used > 0 ? s.stats.guess_residual[s.stats.guess_used]
+                                                     : (have_prev ? s.stats.guess_residual[1] : 1.0);
   T.stats.matvecs[k] = s.stats.matvecs - mv0;
   T.stats.matvecs_fp32[k] = s.stats.matvecs_fp32 - mv32;
   if (rc == EROSION_BREAKDOWN) throw Error(EROSION_BREAKDOWN, "GMRES stalled inside the time step");

@@ -125,8 +125,8 @@ typedef struct {
                            trapezoid rule beyond (where the two agree to
                            rounding); 1 evaluates every pair barycentrically, as
                            deformation_on_boundary does                          */
-  int32_t sweep_decades;/* mixed mode: 0 (default) runs the first refinement sweep
-                           to tol; k > 0 stops every sweep once its estimate has
+  int32_t sweep_decades;/* mixed mode: 0 runs the first refinement sweep to tol;
+                           k > 0 (default 5) stops every sweep once its estimate has
                            fallen 10^-k below the residual it started from (a
                            sweep whose stopping point would lie within a decade
                            of tol runs to tol), and the next sweep restarts from
@@ -135,13 +135,15 @@ typedef struct {
                            relax_tol >= 1 (FP32 far field from the first
                            iteration) the sweeps stay accurate while no FP64
                            far-field sum is needed outside the true residuals      */
-  double relax_tol;     /* mixed mode: GMRES switches to the FP32 far field once its
-                           residual estimate is below relax_tol (relative);
-                           0 selects the library default                           */
+  double relax_tol;     /* mixed mode: GMRES applies the FP32 far field once its
+                           residual estimate is at or below relax_tol ||b||
+                           (default 1: from the first iteration, the refinement
+                           sweeps restoring FP64 accuracy); 0 selects 1e5 tol  */
 } erosion_params;
 
 /* Fills the reference's defaults: wall (3, 1, 8), tol 1e-8, maxl 8000, ibary 1,
- * ifmm 1, ibc 1, FP64, production right-hand side. */
+ * ifmm 1, ibc 1, FP64, production right-hand side; for the mixed mode
+ * (precision 1): fast_fp64 1, relax_tol 1, sweep_decades 5. */
 void erosion_default_params(erosion_params* p);
 
 /* Solve statistics of the last erosion_solve / stokessolver_ call. */
