@@ -513,7 +513,7 @@ bool start_cycle(Member& mb) {
   // as gmres_solve: a mixed-precision cycle stops sweep_decades below its
   // start unless that point lies within a decade of tol
   const int sd = s.pr.P.precision != 0 ? std::max(0, (int)s.pr.P.sweep_decades) : 0;
-  mb.cyc_abs = mb.abs_tol;
+  mb.cyc_abs = (s.pr.P.precision != 0 ? 0.5 : 1.0) * mb.abs_tol;   // a mixed sweep to tol aims at half of it
   if (sd > 0 && mb.r0nrm * std::pow(10.0, -sd) > 10.0 * mb.abs_tol) mb.cyc_abs = mb.r0nrm * std::pow(10.0, -sd);
   ensure_capacity(mb);
   k_copy<<<nblk(N, 256), 256, 0, st>>>(mb.r.p, s.V.p, N);
