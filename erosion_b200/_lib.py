@@ -188,6 +188,7 @@ SIGNATURES = {
                              c_double, PD, PD, PD, PD, PD]),
     "erosion_stream": (ctypes.c_void_p, []),
     "erosion_get_step_density": (c_int, [c_int32, PD, c_int64]),
+    "erosion_get_step_nodes": (c_int, [c_int32, PD, PD, c_int64]),
     "erosion_lw_dims": (c_int, [ctypes.POINTER(c_int32)] * 3),
     "erosion_lw_features": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PF32]),
     "erosion_lw_encode": (c_int, [POINTER(ErosionParams), c_int64, c_int64, c_int64, PD, PD, PD, PF32]),

@@ -1013,12 +1013,13 @@ int gmres_solve(State& s, const double* d_b, double* d_x, bool x0_zero, long lon
   double prev_tr = 1e300;
   const bool mixed = s.pr.P.precision != 0;
   double r_start = x0_zero ? bnrm : device_norm(s, r, N);   // residual the sweep starts from
+  if (!x0_zero) {   // the supplied (or chosen) guess and its residual
+    if (s.stats.guess_used < 1) s.stats.guess_used = 1;
+    s.stats.guess_residual[s.stats.guess_used] = r_start / bnrm;
+  }
   if (!x0_zero && !(r_start < bnrm)) {
-    // An initial guess no better than zero (a previous step's density on a
-    // moved geometry: the large rigid-mode parts of the small bodies no
-    // longer match) would cost iterations just to get back to ||b||; start
-    // from zero instead.
-    s.stats.guess_residual[1] = r_start / bnrm;
+    // An initial guess no better than zero would cost iterations just to get
+    // back to ||b||; start from zero instead.
     EB_CK(cudaMemsetAsync(d_x, 0, N * sizeof(double), st));
     residual(true);
     r_start = bnrm;

@@ -101,6 +101,61 @@ __global__ void k_lw_delta(long long n, const double* __restrict__ x, double* __
   if (i < n) d[i] = x[i] - d[i];
 }
 
+// Warm start across a change of geometry: the previous solve's density,
+// with each body's rigid part carried to the new nodes.  Per body (one
+// block), on the old nodes: t1, t2 = the node means of the two components,
+// t3 = the rotation coefficient about the node mean (xc, yc) (least squares
+// on (-(y - yc), x - xc)); the remainder sigma - rigid stays attached to the
+// node index and the rigid part is evaluated at the new nodes about their
+// own mean.  A rigid-motion density is in the null space of the body's
+// double-layer block, so its size (~6e5 for the smallest bodies of a dense
+// packing) is set by the stokeslet/rotlet rows alone, while the nodes slide
+// along the curves between solves (the theta-L update keeps them at equal
+// arclength): index-aligned, that rigid part leaves a residual of ~1e3 ||b||;
+// carried to the new nodes, ~1e-2 ||b||.  Nodes are at equal arclength, so
+// node means are arclength means.  Wall and stokeslet/rotlet entries are
+// copied unchanged.
+__global__ void __launch_bounds__(TL_NT)
+k_warm_reanchor(int n, int nout, const double* __restrict__ xo, const double* __restrict__ yo,
+                const double* __restrict__ xn, const double* __restrict__ yn, const double* __restrict__ den_old,
+                double* __restrict__ den_new) {
+  __shared__ double red[32];
+  const int b = blockIdx.x;
+  const size_t nodes = (size_t)b * n;
+  const size_t off = 2 * (size_t)nout + 2 * (size_t)n * b;
+  const double* sx = den_old + off;
+  const double* sy = sx + n;
+  double mx = 0, my = 0, mxn = 0, myn = 0, ax = 0, ay = 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    mx += xo[nodes + j]; my += yo[nodes + j];
+    mxn += xn[nodes + j]; myn += yn[nodes + j];
+    ax += sx[j]; ay += sy[j];
+  }
+  mx = block_sum<TL_NT>(mx, red) / n;
+  my = block_sum<TL_NT>(my, red) / n;
+  mxn = block_sum<TL_NT>(mxn, red) / n;
+  myn = block_sum<TL_NT>(myn, red) / n;
+  const double t1 = block_sum<TL_NT>(ax, red) / n;
+  const double t2 = block_sum<TL_NT>(ay, red) / n;
+  double num = 0, den = 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double fx = -(yo[nodes + j] - my), fy = xo[nodes + j] - mx;
+    num += fx * sx[j] + fy * sy[j];
+    den += fx * fx + fy * fy;
+  }
+  num = block_sum<TL_NT>(num, red);
+  den = block_sum<TL_NT>(den, red);
+  const double t3 = den > 0.0 ? num / den : 0.0;
+  double* ox = den_new + off;
+  double* oy = ox + n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double fx = -(yo[nodes + j] - my), fy = xo[nodes + j] - mx;
+    const double gx = -(yn[nodes + j] - myn), gy = xn[nodes + j] - mxn;
+    ox[j] = sx[j] + t3 * (gx - fx);
+    oy[j] = sy[j] + t3 * (gy - fy);
+  }
+}
+
 // xyrot (DensityStress.jl:40): (x, y) -> (-y, x), in place.
 __global__ void k_tl_xyrot(long long nb, double* __restrict__ xx, double* __restrict__ yy) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -284,9 +339,15 @@ struct TL {
   DBuf<double> mterm, nterm, xsd, ysd, atau, tau, xx, yy, tmp;
   DBuf<double> den[2], den_prev;
   long long den_ntot[2] = {-1, -1};
-  // per stage: encoding of the last density increment (learned guess input)
-  DBuf<float> hist[2];
-  bool hist_valid[2] = {false, false};
+  DBuf<double> sx[2], sy[2];   // node coordinates each stage's density was solved on
+  long long s_nodes[2] = {-1, -1};
+  // the most recent solve (either stage): density and node coordinates, the
+  // warm start of the next solve
+  DBuf<double> last_den, last_x, last_y;
+  long long last_ntot = -1;
+  // encoding of the most recent density increment (learned guess input)
+  DBuf<float> hist;
+  bool hist_valid = false;
   DBuf<int> flag, map;
   erosion_step_stats stats{};
 };
@@ -398,17 +459,22 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   T.stats.precond_singular_blocks[k] = s.pc_singular;
   const long long ntot = s.pr.ntot;
   double* den = T.den[k].ensure(ntot);
-  const bool have_prev = sp.warm_start && T.den_ntot[k] == ntot;
+  const bool have_prev = sp.warm_start && T.last_ntot == ntot;
   if (!have_prev) {
     EB_CK(cudaMemsetAsync(den, 0, ntot * sizeof(double), s.st));
-    T.hist_valid[k] = false;
+    T.hist_valid = false;
   } else {
+    // the most recent solve (half a step back), its bodies' rigid parts
+    // carried to this stage's nodes
+    EB_CK(cudaMemcpyAsync(den, T.last_den.p, ntot * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+    k_warm_reanchor<<<M, TL_NT, 0, s.st>>>(n, base.nout, T.last_x.p, T.last_y.p, T.xx.p, T.yy.p, T.last_den.p, den);
+    EB_LAUNCH_CHECK();
     EB_CK(cudaMemcpyAsync(T.den_prev.ensure(ntot), den, ntot * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
   }
   double* rhs = s.d_rhs.ensure(ntot);
   build_rhs(s, rhs);
   const bool zero = choose_initial_guess(s, rhs, den, have_prev, sp.warm_start == 2,
-                                         T.hist_valid[k] ? T.hist[k].p : nullptr);
+                                         T.hist_valid ? T.hist.p : nullptr);
   long long it = 0;
   double est = 0;
   const long long mv0 = s.stats.matvecs, mv32 = s.stats.matvecs_fp32;
@@ -421,12 +487,25 @@ static void stage_derivs(State& s, TL& T, const Problem& base, const erosion_ste
   T.stats.matvecs_fp32[k] = s.stats.matvecs_fp32 - mv32;
   if (rc == EROSION_BREAKDOWN) throw Error(EROSION_BREAKDOWN, "GMRES stalled inside the time step");
   T.den_ntot[k] = ntot;
+  const size_t nbn = (size_t)M * n;
+  EB_CK(cudaMemcpyAsync(T.sx[k].ensure(nbn), T.xx.p, nbn * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+  EB_CK(cudaMemcpyAsync(T.sy[k].ensure(nbn), T.yy.p, nbn * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+  T.s_nodes[k] = (long long)nbn;
+  if (sp.warm_start) {
+    EB_CK(cudaMemcpyAsync(T.last_den.ensure(ntot), den, ntot * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+    EB_CK(cudaMemcpyAsync(T.last_x.ensure(nbn), T.xx.p, nbn * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+    EB_CK(cudaMemcpyAsync(T.last_y.ensure(nbn), T.yy.p, nbn * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+    T.last_ntot = ntot;
+  }
   if (have_prev && sp.warm_start == 2) {
-    // encoding of this step's increment: the next step's network input
+    // encoding of this solve's increment over its warm start: the next
+    // solve's network input
     k_lw_delta<<<nblk(ntot, 256), 256, 0, s.st>>>(ntot, den, T.den_prev.p);
     EB_LAUNCH_CHECK();
-    lw_encode_current(s, T.den_prev.p, T.hist[k].ensure((size_t)M * lw_out_width()));
-    T.hist_valid[k] = true;
+    lw_encode_current(s, T.den_prev.p, T.hist.ensure((size_t)M * lw_out_width()));
+    T.hist_valid = true;
+  } else if (sp.warm_start == 2) {
+    T.hist_valid = false;
   }
   *iters = it;
   *resid = est;
@@ -495,7 +574,8 @@ static int delete_and_compact(State& s, TL& T, int M, int n, double dt1, const d
   }
   EB_CK(cudaStreamSynchronize(s.st));
   T.den_ntot[0] = T.den_ntot[1] = -1;   // body count changed: no warm start
-  T.hist_valid[0] = T.hist_valid[1] = false;
+  T.last_ntot = -1;
+  T.hist_valid = false;
   return Mn;
 }
 
@@ -768,6 +848,20 @@ int erosion_get_step_density(int32_t stage, double* density, int64_t capacity) {
     if (n <= 0) throw Error(EROSION_BAD_INPUT, "no solved density of that stage since the last body-count change");
     if (capacity < n) throw Error(EROSION_BAD_INPUT, "density capacity below the stage's unknown count");
     d2h(density, T.den[stage].p, n, s.st);
+    EB_CK(cudaStreamSynchronize(s.st));
+    return EROSION_OK;
+  });
+}
+
+int erosion_get_step_nodes(int32_t stage, double* xx, double* yy, int64_t capacity) {
+  return guarded3([&](State& s) {
+    TL& T = tl();
+    if (stage < 0 || stage > 1 || !xx || !yy) throw Error(EROSION_BAD_INPUT, "stage must be 0 or 1");
+    if (T.den_ntot[stage] <= 0) throw Error(EROSION_BAD_INPUT, "no solve of that stage since the last body-count change");
+    const long long nb = T.s_nodes[stage];
+    if (capacity < nb) throw Error(EROSION_BAD_INPUT, "node capacity below the stage's node count");
+    d2h(xx, T.sx[stage].p, nb, s.st);
+    d2h(yy, T.sy[stage].p, nb, s.st);
     EB_CK(cudaStreamSynchronize(s.st));
     return EROSION_OK;
   });

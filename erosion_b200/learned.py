@@ -1,17 +1,21 @@
 """The learned initial guess from Python: training sets from the solver's own
 erosion runs, and training, through the C ABI (erosion_lw_*).
 
-The network (learned.cu) predicts, per body, the encoding of the density's
-increment over one time step from the body's geometry features and the
-encoding of its previous increment; the guess of an erosion step with
-warm_start = 2 is the previous step's density plus that prediction.  A
-training row is therefore
+An erosion run solves twice per RK2 step (the state, then the half-step
+state); each solve's warm start is the previous solve's density with every
+body's rigid part carried to the new nodes (`reanchor`, the same arithmetic
+as the library's k_warm_reanchor).  The network (learned.cu) predicts, per
+body, the encoding of the increment of the density over that warm start from
+the body's geometry features and the encoding of the previous solve's
+increment; with warm_start = 2 the candidate guess is the warm start plus
+that prediction.  A training row is therefore, for consecutive solves
+i-2, i-1, i with unchanged body count,
 
-    X = [geometry features of step k (68) | encoding of x_{k-1} - x_{k-2} (37)]
-    Y = encoding of x_k - x_{k-1} (37)
+    X = [geometry features of solve i (68) | encoding of d_{i-1} on solve i-1's nodes (37)]
+    Y = encoding of d_i on solve i's nodes (37)
 
-with x_k the density solved in the first stage of step k (on the state the
-step starts from), all on the geometry of step k.
+with d_i = x_i - reanchor(x_{i-1}) the increment of solve i over its warm
+start.
 """
 from __future__ import annotations
 
@@ -56,11 +60,34 @@ def getxy(n, M, th, ln, xs, ys):
     return xx, yy
 
 
+def reanchor(n, nout, xo, yo, xn, yn, den):
+    """The previous solve's density carried to new nodes: per body, the rigid
+    part (node means t1, t2 of the two components; rotation coefficient t3
+    about the node mean, least squares on (-(y - yc), x - xc)) is evaluated
+    at the new nodes about their own mean, the remainder stays attached to
+    the node index; wall and stokeslet/rotlet entries unchanged."""
+    den = np.asarray(den, dtype=np.float64)
+    out = den.copy()
+    M = len(xo) // n
+    xo, yo = np.asarray(xo).reshape(M, n), np.asarray(yo).reshape(M, n)
+    xn, yn = np.asarray(xn).reshape(M, n), np.asarray(yn).reshape(M, n)
+    for b in range(M):
+        off = 2 * nout + 2 * n * b
+        sx, sy = den[off:off + n], den[off + n:off + 2 * n]
+        fx, fy = -(yo[b] - yo[b].mean()), xo[b] - xo[b].mean()
+        gx, gy = -(yn[b] - yn[b].mean()), xn[b] - xn[b].mean()
+        dd = (fx * fx + fy * fy).sum()
+        t3 = (fx * sx + fy * sy).sum() / dd if dd > 0 else 0.0
+        out[off:off + n] = sx + t3 * (gx - fx)
+        out[off + n:off + 2 * n] = sy + t3 * (gy - fy)
+    return out
+
+
 def trajectory(params, sp, n, nout, th, ln, xs, ys, steps: int):
     """Runs `steps` RK2 erosion steps (erosion_rk2_step, host arrays, updated
-    in place) and returns per step the state's node coordinates and the
-    density solved in its first stage: a list of (xx, yy, density, M), with
-    None where a body was deleted during the step."""
+    in place) and returns every solve in order, two per step: (xx, yy,
+    density, M) of the nodes and density of each stage, with None for the
+    solves of a step in which a body was deleted."""
     L = _lib.load()
     M = len(ln)
     nb = np.array([M], np.int64)
@@ -69,31 +96,39 @@ def trajectory(params, sp, n, nout, th, ln, xs, ys, steps: int):
     out = []
     for _ in range(steps):
         Mk = int(nb[0])
-        xx, yy = getxy(n, Mk, th[: Mk * n], ln[:Mk], xs[:Mk], ys[:Mk])
         rc = L.erosion_rk2_step(ctypes.byref(params), ctypes.byref(sp), n, nb.ctypes.data_as(PI64), nout, ptr(th),
                                 ptr(ln), ptr(xs), ptr(ys), ptr(t), dele.ctypes.data_as(PI64))
         check(rc, (_lib.EROSION_OK, _lib.EROSION_MAXITER))
         if int(nb[0]) != Mk:
-            out.append(None)
+            out += [None, None]
             continue
-        den = np.zeros(2 * nout + 2 * n * Mk + 3 * Mk)
-        check(L.erosion_get_step_density(0, ptr(den), den.size))
-        out.append((xx, yy, den, Mk))
+        for stage in (0, 1):
+            den = np.zeros(2 * nout + 2 * n * Mk + 3 * Mk)
+            xx, yy = np.zeros(n * Mk), np.zeros(n * Mk)
+            check(L.erosion_get_step_density(stage, ptr(den), den.size))
+            check(L.erosion_get_step_nodes(stage, ptr(xx), ptr(yy), xx.size))
+            out.append((xx, yy, den, Mk))
     return out
 
 
 def training_rows(params, n, nout, traj):
-    """(X, Y) rows of consecutive triples of a trajectory (see the module
-    docstring); triples that cross a body deletion are skipped."""
+    """(X, Y) rows of consecutive solve triples of a trajectory (see the
+    module docstring); triples that cross a body deletion are skipped."""
     X, Y = [], []
-    for k in range(2, len(traj)):
-        a, b, c = traj[k - 2], traj[k - 1], traj[k]
-        if a is None or b is None or c is None or not (a[3] == b[3] == c[3]):
+    inc = [None] * len(traj)
+    for i in range(1, len(traj)):
+        a, b = traj[i - 1], traj[i]
+        if a is None or b is None or a[3] != b[3]:
             continue
-        xx, yy, den, M = c
+        inc[i] = b[2] - reanchor(n, nout, a[0], a[1], b[0], b[1], a[2])
+    for i in range(2, len(traj)):
+        if inc[i] is None or inc[i - 1] is None:
+            continue
+        xx, yy, _, M = traj[i]
+        px, py = traj[i - 1][0], traj[i - 1][1]
         f = features(params, n, M, nout, xx, yy)
-        hist = encode(params, n, M, nout, xx, yy, b[2] - a[2])
-        targ = encode(params, n, M, nout, xx, yy, den - b[2])
+        hist = encode(params, n, M, nout, px, py, inc[i - 1])
+        targ = encode(params, n, M, nout, xx, yy, inc[i])
         X.append(np.concatenate([f, hist], 1))
         Y.append(targ)
     if not X:

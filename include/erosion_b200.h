@@ -327,10 +327,13 @@ typedef struct {
                            (DensityStress.jl:129-167; meaningful for walls
                            that contain those slices)                            */
   int32_t warm_start;   /* 0: zero initial guess (the reference,
-                           DensityStress.jl:45); 1: previous solve's density of
-                           the same stage when the body count is unchanged;
-                           2: as 1 plus the learned guess, whichever of the
-                           candidates has the smallest residual                  */
+                           DensityStress.jl:45); 1: the most recent solve's
+                           density (the other stage, half a step back) when
+                           the body count is unchanged, each body's rigid part
+                           carried to the new nodes; 2: as 1 plus the learned
+                           increment, whichever candidate has the smallest
+                           residual.  In the mixed or preconditioned solve a
+                           guess no better than zero is replaced by zero      */
   int32_t reserved[5];
 } erosion_step_params;
 
@@ -384,6 +387,11 @@ void erosion_get_step_stats(erosion_step_stats* s);
  * started from.  EROSION_BAD_INPUT when there is none (no step yet, or the
  * body count changed after the solve). */
 int erosion_get_step_density(int32_t stage, double* density, int64_t capacity);
+
+/* The body node coordinates that density was solved on (npts*nbods each;
+ * stage 1's nodes are those of the half-step state, which the caller does
+ * not otherwise see). */
+int erosion_get_step_nodes(int32_t stage, double* xx, double* yy, int64_t capacity);
 
 /* Drag on the bodies of a theta-L state: replaces drag (PostProcess.jl:131-162)
  * with the shear stress and pressure it calls (compute_stress,
