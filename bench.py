@@ -82,7 +82,7 @@ TRAFFIC_BYTES_PER_NODE = {"k_far32": (11398144 + 16384) / 106496, "k_far64_fast"
 # leg of this script measures them on the GPU.  Used only by the reference
 # arm's model for workloads whose CPU solve cannot finish in minutes; on c1
 # the reference arm runs the oracle's own GMRES instead.
-PLAIN_ITERATIONS_PER_STEP = {"c2": 3165, "c3": 12046}
+PLAIN_ITERATIONS_PER_STEP = {"c2": 3165, "c3": 13436}
 
 
 def parse(argv=None):

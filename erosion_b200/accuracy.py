@@ -58,6 +58,7 @@ def main(argv=None):
     t = np.zeros(1)
     dele = np.zeros(g0.M, np.int64)
     x64 = None
+    prev_xy = None
     worst = {"density": 0.0, "pressure_drop": 0.0, "shear_stress": 0.0}
     for k in range(args.steps):
         M = int(nb[0])
@@ -65,6 +66,9 @@ def main(argv=None):
         g = G.Geometry(n, nout, xx, yy, g0.wall, g0.ibc, np.zeros(M), np.zeros((M, 2)))
         if x64 is not None and len(x64) != g.ntot:
             x64 = None
+        if x64 is not None:   # the previous step's solution, rigid parts carried to the new nodes
+            x64 = learned.reanchor(n, nout, prev_xy[0], prev_xy[1], xx, yy, x64)
+        prev_xy = (xx, yy)
         t0 = time.perf_counter()
         x64, it64, s64 = stokes.solve(g, x0=x64, tol=args.ref_tol, precision=0, precond=1, maxl=4000,
                                       allow=(0, 1))
