@@ -25,6 +25,13 @@ void set_status(int code, const std::string& msg) {
 static int g_num_sms = 148;
 int eb_num_sms() { return g_num_sms; }
 
+void allow_max_dynamic_smem(const void* fn) {
+  int dev = 0, optin = 0;
+  EB_CK(cudaGetDevice(&dev));
+  EB_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  EB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+}
+
 void ensure_init(State& s) {
   if (s.init) return;
   int ndev = 0;
@@ -629,14 +636,12 @@ void setup_preconditioner(State& s) {
   while (pb > 4 && gj_smem(pb) > 200 * 1024) pb /= 2;
   if (gj_smem(pb) <= 200 * 1024) {
     const size_t smem = gj_smem(pb);
-    if (smem > 48 * 1024)
-      EB_CK(cudaFuncSetAttribute(k_gj_inv32_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32_blocked);
     k_gj_inv32_blocked<<<pr.M, 512, smem, s.st>>>(m, pb, B, bad);
     EB_LAUNCH_CHECK();
   } else {
     const size_t smem = 3 * (size_t)m * sizeof(float);
-    if (smem > 48 * 1024)
-      EB_CK(cudaFuncSetAttribute(k_gj_inv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32);
     k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
     EB_LAUNCH_CHECK();
   }

@@ -189,6 +189,11 @@ struct State {
 
 State& state();
 int eb_num_sms();
+// Raises a kernel's dynamic shared-memory cap to the device's opt-in maximum.
+// Every caller sets the same value, so set-ups running concurrently on host
+// threads (the ensemble) that need different sizes never lower the cap under
+// each other's launches.
+void allow_max_dynamic_smem(const void* fn);
 // The outcome of the last entry-point call made by the calling thread,
 // read back by erosion_last_status / erosion_last_error.  Thread-local, so it
 // takes no lock and one thread's call never overwrites another's outcome.

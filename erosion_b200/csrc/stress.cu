@@ -740,7 +740,7 @@ void shear_stress(State& s, const double* d_den, double* d_tau, double* d_E) {
   static DBuf<int> d_sc;
   eself.ensure(3LL * nb);
   size_t smem = 7 * (size_t)pr.n * sizeof(double);
-  if (smem > 48 * 1024) EB_CK(cudaFuncSetAttribute(k_stress_self, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_stress_self);
   k_stress_self<<<pr.M, 256, smem, s.st>>>(G, d_den, s.dker_body.p, eself.p);
   EB_LAUNCH_CHECK();
   const int bary = pr.P.ibary == 1;

@@ -92,3 +92,16 @@ def test_batch_iteration_cap(lib, ens):
                                         allow=(_lib.EROSION_OK, _lib.EROSION_MAXITER))
     assert (nits <= 5).all()
     assert _lib.load().erosion_last_status() == _lib.EROSION_MAXITER
+
+
+def test_batch_members_with_different_block_sizes(lib):
+    """Members whose preconditioner blocks need different shared-memory
+    sizes (128, 256 and 512 nodes per body: blocks of 259, 515 and 1027) are
+    set up concurrently on host threads; each launch must still get the
+    shared memory it asks for."""
+    ens = [G.ensemble(1, seed=40 + k, bodies=(2, 3), npts=(n,), porosity=(0.9, 0.9), nout=256)[0]
+           for k, n in enumerate((128, 512, 256, 512, 128, 256))]
+    dens, nits, st = stokes.solve_batch(ens, tol=1e-10, precond=1)
+    for g, d in zip(ens, dens):
+        ref, _, _ = stokes.solve(g, tol=1e-10, precond=1)
+        assert rel(d, ref) < 1e-8
