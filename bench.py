@@ -391,9 +391,10 @@ def run_ensemble(args, world, rank, local, dist):
 # ---------------------------------------------------------------------------
 def run_learned(args, world, rank, local, dist):
     """The learned warm start (workload c5): trains the increment network on
-    the first-stage densities of a 400-body run (c3 shapes, a different seed),
-    then erodes a 200-body, 256-node channel until half of its body area is
-    gone, once with the previous step's density as the GMRES initial guess
+    the solves of a 400-body run (c3 shapes, a different seed; both stages of
+    every step, increments over their carried-over warm starts), then erodes
+    a 200-body, 256-node channel until half of its body area is gone, once
+    with the carried-over previous solve as the GMRES initial guess
     (warm_start = 1) and once with the learned guess (warm_start = 2), both
     mixed precision + block preconditioner to 1e-8.  dt is set from a first
     step so that the run takes about --c5-steps steps.  value = erosion steps/s
@@ -429,7 +430,7 @@ def run_learned(args, world, rank, local, dist):
     rate = max((A0 - float(learned.areas(n, th[: int(nb[0]) * n], ln[: nb[0]], xs[: nb[0]], ys[: nb[0]]).sum()))
                / dt0, 1e-12)
     dt = 0.5 * A0 / rate / max(args.c5_steps, 1)
-    # training set: first-stage densities of a 400-body run at the same dt
+    # training set: the solves of a 400-body run at the same dt
     g3 = G.workload("c3", seed=args.seed + 1)
     t3 = [a.copy() for a in G.to_thetalen(g3)]
     t_train0 = time.perf_counter()
@@ -490,9 +491,10 @@ def run_learned(args, world, rank, local, dist):
                                                                       f"{args.c5_steps} steps (from one probe step)",
                            "tol": 1e-8, "precision": "mixed" if args.precision else "fp64",
                            "precond": "block Gauss-Seidel" if args.precond else "none",
-                           "training": {"rows": int(len(X)), "source": f"first-stage densities of "
+                           "training": {"rows": int(len(X)), "source": f"per-body increments of the two solves of each of "
                                                                        f"{args.train_steps} steps of a 400-body "
-                                                                       f"run (c3 shapes, seed {args.seed + 1})",
+                                                                       f"run (c3 shapes, seed {args.seed + 1}), "
+                                                                       f"over their carried-over warm starts",
                                         "epochs": 300, "mse_first_epoch": loss0, "mse_last_epoch": loss,
                                         "seconds": t_train}},
                 "previous_step": {k: v for k, v in prev.items() if k != "record"},
