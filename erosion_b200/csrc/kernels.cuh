@@ -1596,12 +1596,6 @@ __global__ void k_bminus(const double* __restrict__ b, double* __restrict__ r, l
   if (i < n) r[i] = b[i] - r[i];
 }
 
-// Wall entries of x += -2 r (Richardson step with the wall block's -1/2 I).
-__global__ void k_wall_richardson(int nout, const double* __restrict__ r, double* __restrict__ x) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < 2 * nout) x[i] += -2.0 * r[i];
-}
-
 // y += a x
 __global__ void k_axpy(double a, const double* __restrict__ x, double* __restrict__ y, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;

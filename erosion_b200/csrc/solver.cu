@@ -29,7 +29,9 @@ void allow_max_dynamic_smem(const void* fn) {
   int dev = 0, optin = 0;
   EB_CK(cudaGetDevice(&dev));
   EB_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  EB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  cudaFuncAttributes fa;
+  EB_CK(cudaFuncGetAttributes(&fa, fn));   // the cap excludes the kernel's static shared memory
+  EB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
 }
 
 void ensure_init(State& s) {
@@ -553,6 +555,54 @@ void record_setup_stats(State& s) {
   s.stats.ms_precond_setup = s.pc_setup_ms;
 }
 
+// The wall's own state (no bodies): its operator is the wall block A_ww of
+// the full operator (wall sources at wall targets with the rank-one term).
+static State& wall_state() {
+  static State w;
+  return w;
+}
+
+// Wall part of a candidate density given its bodies: c_wall += A_ww^{-1} r_wall
+// for the residual r = b - A c of the full problem.  The body and wall
+// densities carry fields that cancel against each other, so a body-only
+// update of a density (the learned increment) is useless without the wall's
+// answer to it (measured with the oracle on a 10-body channel: the exact body
+// increment without the wall's raised the residual 25-fold; with the wall
+// rows solved for, it lowered it 28-fold).  A_ww = -1/2 I + D_ww + the
+// rank-one term is well conditioned (condition ~40 at 1024 wall nodes):
+// plain FP64 GMRES to 1e-6 takes a few tens of iterations of an N_out^2 sum.
+static void solve_wall_rows(State& s, const double* d_r, double* d_c) {
+  State& w = wall_state();
+  ensure_init(w);
+  const Problem& pr = s.pr;
+  const long long nw = 2LL * pr.nout;
+  const bool same = w.geo_valid && w.pr.nout == pr.nout && w.pr.P.wall_a == pr.P.wall_a &&
+                    w.pr.P.wall_b == pr.P.wall_b && w.pr.P.wall_order == pr.P.wall_order &&
+                    w.pr.P.ibary == pr.P.ibary && w.pr.P.ifmm == pr.P.ifmm;
+  EB_CK(cudaStreamSynchronize(s.st));   // r is complete before the wall state's stream reads it
+  if (!same) {
+    Problem pw = pr;
+    pw.M = 0;
+    pw.n = 2;
+    pw.P.precision = 0;
+    pw.P.precond = 0;
+    pw.P.learned_guess = 0;
+    pw.P.true_residual = 0;
+    setup_problem(w, pw, w.d_xx.ensure(1), w.d_yy.ensure(1));
+  }
+  double* rb = w.d_rhs.ensure(nw);
+  double* dx = w.d_den.ensure(nw);
+  EB_CK(cudaMemcpyAsync(rb, d_r, nw * sizeof(double), cudaMemcpyDeviceToDevice, w.st));
+  EB_CK(cudaMemsetAsync(dx, 0, nw * sizeof(double), w.st));
+  long long it = 0;
+  double est = 0;
+  const int rc = gmres_solve(w, rb, dx, true, 200, 1e-6, &it, &est);
+  if (rc == EROSION_BREAKDOWN) return;   // leave the candidate's wall part as it is
+  k_axpy<<<nblk(nw, 256), 256, 0, w.st>>>(1.0, dx, d_c, nw);
+  EB_LAUNCH_CHECK();
+  EB_CK(cudaStreamSynchronize(w.st));
+}
+
 bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x, bool learned, const float* d_hist) {
   for (int q = 0; q < 3; ++q) s.stats.guess_residual[q] = -1.0;
   s.stats.guess_residual[0] = 1.0;
@@ -582,13 +632,10 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
   double* c = cand.ensure(N);
   if (have_x) EB_CK(cudaMemcpyAsync(c, d_x, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
   if (have_x && lw_guess_increment(s, d_hist, c)) {
-    // the network predicts the bodies' increment only: update the wall
-    // density by one Richardson sweep on the wall rows (wall block ~ -1/2 I)
-    for (int it = 0; it < 1; ++it) {
-      rel_res(c);
-      k_wall_richardson<<<nblk(2LL * s.pr.nout, 256), 256, 0, st>>>(s.pr.nout, r, c);
-      EB_LAUNCH_CHECK();
-    }
+    // the network predicts the bodies' increment only: the wall's part
+    // follows from the wall rows given the new body densities
+    rel_res(c);
+    solve_wall_rows(s, r, c);
     const double rl = rel_res(c);
     s.stats.guess_residual[2] = rl;
     if (rl < best) {
@@ -1395,6 +1442,7 @@ void erosion_release(void) {
   std::lock_guard<std::mutex> lk(s.mu);
   release_batch();
   release_state_buffers(s);
+  release_state_buffers(wall_state());
 }
 
 }  // extern "C"

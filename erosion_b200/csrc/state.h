@@ -189,8 +189,8 @@ struct State {
 
 State& state();
 int eb_num_sms();
-// Raises a kernel's dynamic shared-memory cap to the device's opt-in maximum.
-// Every caller sets the same value, so set-ups running concurrently on host
+// Raises a kernel's dynamic shared-memory cap to the device's opt-in maximum
+// (less the kernel's static shared memory).  Every caller sets the same value, so set-ups running concurrently on host
 // threads (the ensemble) that need different sizes never lower the cap under
 // each other's launches.
 void allow_max_dynamic_smem(const void* fn);
