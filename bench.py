@@ -446,7 +446,8 @@ def run_learned(args, world, rank, local, dist):
         t = np.zeros(1)
         dele = np.zeros(g5.M, np.int64)
         sp = sparams(dt, ws)
-        rec = {"iterations": [], "ms": [], "guess_used": [], "guess_residual": [], "bodies": [], "area_frac": []}
+        rec = {"iterations": [], "ms": [], "guess_used": [], "guess_residual": [], "bodies": [], "area_frac": [],
+               "candidates_last_solve": []}
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         area = A0
@@ -468,6 +469,8 @@ def run_learned(args, world, rank, local, dist):
             rec["ms"].append(e0.elapsed_time(e1))
             rec["guess_used"].append(d["guess_used"])
             rec["guess_residual"].append(d["guess_residual"])
+            # the step's second solve: residuals of its candidates (zero, warm start, learned; -1 not tried)
+            rec["candidates_last_solve"].append(_lib.solve_stats()["guess_residual"])
             rec["bodies"].append(M)
             rec["area_frac"].append(area / A0)
         steps = len(rec["ms"])

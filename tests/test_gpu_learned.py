@@ -97,7 +97,7 @@ def test_training_and_learned_guess_gain(lib):
         nb = np.array([g2.M], np.int64)
         t = np.zeros(1)
         dele = np.zeros(g2.M, np.int64)
-        its, res, used = [], [], []
+        its, res, used, cand = [], [], [], []
         for k in range(12):
             rc = lib.erosion_rk2_step(ctypes.byref(p), ctypes.byref(sp), g2.n, nb.ctypes.data_as(_lib.PI64), g2.nout,
                                       _lib.ptr(th), _lib.ptr(ln), _lib.ptr(xs), _lib.ptr(ys),
@@ -111,9 +111,11 @@ def test_training_and_learned_guess_gain(lib):
                 its.append(sum(d["gmres_iterations"]))
                 res.append(np.mean(d["guess_residual"]))
                 used.append(d["guess_used"])
-        runs[ws] = (np.mean(its), np.mean(res), used)
+                cand.append(_lib.solve_stats()["guess_residual"][2])   # learned candidate, second solve
+        runs[ws] = (np.mean(its), np.mean(res), used, cand)
     assert all(u in (1, 2) for pair in runs[2][2] for u in pair)
     print(f"training MSE {loss0:.3f} -> {loss:.3f}; initial residual previous-step {runs[1][1]:.3g} vs learned "
           f"{runs[2][1]:.3g}; iterations per step {runs[1][0]:.1f} vs {runs[2][0]:.1f}; learned used "
-          f"{sum(u == 2 for pair in runs[2][2] for u in pair)} of {2 * len(runs[2][2])} stages")
+          f"{sum(u == 2 for pair in runs[2][2] for u in pair)} of {2 * len(runs[2][2])} stages; learned candidate "
+          f"residual {np.mean(runs[2][3]):.3g}")
     assert runs[2][0] <= runs[1][0] + 2
