@@ -293,7 +293,7 @@ def far_shapes() -> dict:
         if kind != 1:
             label = lambda c: f"{c[0]}x{c[1]}-{RCP_LABELS.get(c[2], c[2])}"
         else:
-            label = lambda c: f"{c[0]}x{c[1]}-unroll{c[2]}"
+            label = lambda c: f"{c[0]}x{c[1]}-unroll{c[2] % 10}-{c[2] // 10}cta"
         out[name] = {"shape": label(cands[shape[kind]]), "index": shape[kind],
                      "tuned_ms": {label(c): round(ms[8 * kind + i], 4) for i, c in enumerate(cands)}}
     return out

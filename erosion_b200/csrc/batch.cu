@@ -223,16 +223,16 @@ void launch_batch64(Batch& B, int shape, int njobs, long long items, cudaStream_
 
 void launch_batch32(Batch& B, int shape, int njobs, long long items, cudaStream_t st) {
   if (njobs == 0) return;
-#define EB_B32(IDX, NT, TPT, U)                                                                        \
+#define EB_B32(IDX, NT, TPT, U, MB)                                                                        \
   case IDX: {                                                                                          \
-    k_far32_batch<NT, TPT, U><<<persistent_grid(B.occ32[IDX], items), NT, 0, st>>>(B.jobs32.p, njobs, items); \
+    k_far32_batch<NT, TPT, U, MB><<<persistent_grid(B.occ32[IDX], items), NT, 0, st>>>(B.jobs32.p, njobs, items); \
     break;                                                                                             \
   }
   switch (shape) {
-    EB_B32(0, 256, 4, 2)
-    EB_B32(1, 256, 4, 4)
-    EB_B32(2, 256, 2, 2)
-    EB_B32(3, 256, 2, 4)
+    EB_B32(0, 256, 4, 2, 2)
+    EB_B32(1, 256, 4, 4, 2)
+    EB_B32(2, 256, 4, 2, 3)
+    EB_B32(3, 256, 4, 4, 3)
     default: throw Error(EROSION_BAD_INPUT, "unknown FP32 batch shape");
   }
 #undef EB_B32
@@ -244,7 +244,8 @@ static_assert(kFar64Shapes[0].nt == 256 && kFar64Shapes[0].tpt == 2 && kFar64Sha
               kFar64Shapes[2].nt == 256 && kFar64Shapes[2].tpt == 2 && kFar64Shapes[2].rcp == 3 &&
               kFar64Shapes[3].nt == 128 && kFar64Shapes[3].tpt == 4 && kFar64Shapes[3].rcp == 3 &&
               kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
-              kFar32Shapes[2].nt == 256 && kFar32Shapes[2].tpt == 2 && kFar32Shapes[3].rcp == 4,
+              kFar32Shapes[2].minb == 3 && kFar32Shapes[2].tpt == 4 && kFar32Shapes[3].rcp == 4 &&
+              kFar32Shapes[3].minb == 3,
               "launch_batch shape tables");
 
 // Chooses the ensemble launch shapes by timing each candidate on the jobs of
@@ -254,10 +255,10 @@ void occupancy(Batch& B) {
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[1], k_far64_batch<128, 4, 1>, 128, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[2], k_far64_batch<256, 2, 3>, 256, 0));
   EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ64[3], k_far64_batch<128, 4, 3>, 128, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[0], k_far32_batch<256, 4, 2>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[1], k_far32_batch<256, 4, 4>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[2], k_far32_batch<256, 2, 2>, 256, 0));
-  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[3], k_far32_batch<256, 2, 4>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[0], k_far32_batch<256, 4, 2, 2>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[1], k_far32_batch<256, 4, 4, 2>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[2], k_far32_batch<256, 4, 2, 3>, 256, 0));
+  EB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B.occ32[3], k_far32_batch<256, 4, 4, 3>, 256, 0));
 }
 
 void tune_batch(Batch& B, double pairs_total) {

@@ -519,13 +519,10 @@ __device__ __forceinline__ void far32_cta(int N, int nout, int n, const float4* 
   }
 }
 
-// Resident CTAs per SM the FP32 far field is compiled for: two lane pairs
-// of targets per thread (TPT = 4) need more registers than one (TPT = 2),
-// which is compiled for half as many warps again per SM.
-__host__ __device__ constexpr int far32_min_blocks(int nt, int tpt) { return (tpt <= 2 ? 768 : 512) / nt; }
-
-template <bool MASK, int NT, int TPT, int U>
-__global__ void __launch_bounds__(NT, far32_min_blocks(NT, TPT))
+// MINB: resident CTAs per SM the kernel is compiled for (the register
+// budget: 2 CTAs of 256 threads leave 128 registers a thread, 3 leave 85).
+template <bool MASK, int NT, int TPT, int U, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
 k_far32(int N, int nout, int n, const float4* __restrict__ src, const float2* __restrict__ tgt,
         const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float4* __restrict__ sq32,
         const int4* __restrict__ tiles, const int* __restrict__ split_ptr, const unsigned* __restrict__ mask, int mw,
@@ -595,8 +592,8 @@ k_far64_batch(const FarJob64* __restrict__ jobs, int njobs, long long nitems) {
   }
 }
 
-template <int NT, int TPT, int U>
-__global__ void __launch_bounds__(NT, far32_min_blocks(NT, TPT))
+template <int NT, int TPT, int U, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
 k_far32_batch(const FarJob32* __restrict__ jobs, int njobs, long long nitems) {
   __shared__ float4 s_pos[F32_TS];
   __shared__ float4 s_q1[F32_TS];
@@ -618,11 +615,13 @@ k_far32_batch(const FarJob32* __restrict__ jobs, int njobs, long long nitems) {
 // Launch shapes the autotuner chooses from (threads per CTA, targets per
 // thread); solver.cu times each on the geometry at hand.
 // The third field is a kernel variant: for the FP64 kernels the reciprocal
-// (rcp_variant), for the FP32 kernel the unroll factor of the source loop.
+// (rcp_variant), for the FP32 kernel the unroll factor of the source loop;
+// the fourth, for the FP32 kernel, the resident CTAs per SM it is compiled
+// for (TPT = 4 fits 80 registers without spills at 3 CTAs of 256 threads).
 // Kinds: 0 accurate FP64 (reciprocal at FP64 rounding), 1 FP32, 2 fast FP64.
-struct FarShape { int nt, tpt, rcp; };
+struct FarShape { int nt, tpt, rcp, minb; };
 constexpr FarShape kFar64Shapes[] = {{256, 2, 1}, {128, 4, 1}, {256, 2, 3}, {128, 4, 3}};
-constexpr FarShape kFar32Shapes[] = {{256, 4, 2}, {256, 4, 4}, {256, 2, 2}, {256, 2, 4}};
+constexpr FarShape kFar32Shapes[] = {{256, 4, 2, 2}, {256, 4, 4, 2}, {256, 4, 2, 3}, {256, 4, 4, 3}};
 constexpr FarShape kFar64FastShapes[] = {{256, 2, 2}, {128, 4, 2}, {256, 2, 4}, {128, 4, 4}};
 constexpr int kNumFar64Shapes = 4, kNumFar32Shapes = 4, kNumFar64FastShapes = 4;
 constexpr int kFarKinds = 3;

@@ -289,9 +289,13 @@ static_assert(kFar64FastShapes[0].nt == 256 && kFar64FastShapes[0].tpt == 2 && k
               kFar64FastShapes[3].nt == 128 && kFar64FastShapes[3].tpt == 4 && kFar64FastShapes[3].rcp == 4,
               "launch_far's fast FP64 cases");
 static_assert(kFar32Shapes[0].nt == 256 && kFar32Shapes[0].tpt == 4 && kFar32Shapes[0].rcp == 2 &&
+                  kFar32Shapes[0].minb == 2 &&
               kFar32Shapes[1].nt == 256 && kFar32Shapes[1].tpt == 4 && kFar32Shapes[1].rcp == 4 &&
-              kFar32Shapes[2].nt == 256 && kFar32Shapes[2].tpt == 2 && kFar32Shapes[2].rcp == 2 &&
-              kFar32Shapes[3].nt == 256 && kFar32Shapes[3].tpt == 2 && kFar32Shapes[3].rcp == 4,
+                  kFar32Shapes[1].minb == 2 &&
+              kFar32Shapes[2].nt == 256 && kFar32Shapes[2].tpt == 4 && kFar32Shapes[2].rcp == 2 &&
+                  kFar32Shapes[2].minb == 3 &&
+              kFar32Shapes[3].nt == 256 && kFar32Shapes[3].tpt == 4 && kFar32Shapes[3].rcp == 4 &&
+                  kFar32Shapes[3].minb == 3,
               "launch_far's FP32 cases");
 
 // One far-field launch of the given kind (0 accurate FP64 and 2 fast FP64 on
@@ -304,14 +308,14 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
   cudaStream_t st = s.st;
   const bool mk = nr.npairs > 0;
   const dim3 g((unsigned)nblk(pr.N, shape_targets(kind, shape)), (unsigned)nsplit);
-#define EB_FAR32(IDX, NT, TPT, U)                                                                                 \
+#define EB_FAR32(IDX, NT, TPT, U, MB)                                                                           \
   case IDX:                                                                                                       \
     if (mk)                                                                                                       \
-      k_far32<true, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p, s.tile_c.p, \
-                                               s.sq32.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);           \
+      k_far32<true, NT, TPT, U, MB><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,        \
+                                                   s.tile_c.p, s.sq32.p, s.tiles.p, sp, nr.mask.p, nr.mw, out);  \
     else                                                                                                          \
-      k_far32<false, NT, TPT, U><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,           \
-                                                s.tile_c.p, s.sq32.p, s.tiles.p, sp, nullptr, 0, out);    \
+      k_far32<false, NT, TPT, U, MB><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,       \
+                                                    s.tile_c.p, s.sq32.p, s.tiles.p, sp, nullptr, 0, out);     \
     break;
 #define EB_FAR64(IDX, NT, TPT, RCP)                                                                          \
   case IDX:                                                                                                  \
@@ -322,10 +326,10 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
     break;
   if (kind == 1) {
     switch (shape) {
-      EB_FAR32(0, 256, 4, 2)
-      EB_FAR32(1, 256, 4, 4)
-      EB_FAR32(2, 256, 2, 2)
-      EB_FAR32(3, 256, 2, 4)
+      EB_FAR32(0, 256, 4, 2, 2)
+      EB_FAR32(1, 256, 4, 4, 2)
+      EB_FAR32(2, 256, 4, 2, 3)
+      EB_FAR32(3, 256, 4, 4, 3)
       default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
     }
   } else if (kind == 0) {
@@ -355,9 +359,9 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
 static int far_resident(int kind, int shape, bool masked) {
   const void* fn = nullptr;
   int nt = 0;
-#define EB_R32(IDX, NT, TPT, U)                                                                          \
+#define EB_R32(IDX, NT, TPT, U, MB)                                                                      \
   case IDX:                                                                                             \
-    fn = masked ? (const void*)k_far32<true, NT, TPT, U> : (const void*)k_far32<false, NT, TPT, U>;     \
+    fn = masked ? (const void*)k_far32<true, NT, TPT, U, MB> : (const void*)k_far32<false, NT, TPT, U, MB>; \
     nt = NT;                                                                                            \
     break;
 #define EB_R64(IDX, NT, TPT, RCP)                                                                        \
@@ -366,7 +370,7 @@ static int far_resident(int kind, int shape, bool masked) {
     nt = NT;                                                                                            \
     break;
   if (kind == 1) {
-    switch (shape) { EB_R32(0, 256, 4, 2) EB_R32(1, 256, 4, 4) EB_R32(2, 256, 2, 2) EB_R32(3, 256, 2, 4) default: break; }
+    switch (shape) { EB_R32(0, 256, 4, 2, 2) EB_R32(1, 256, 4, 4, 2) EB_R32(2, 256, 4, 2, 3) EB_R32(3, 256, 4, 4, 3) default: break; }
   } else if (kind == 0) {
     switch (shape) { EB_R64(0, 256, 2, 1) EB_R64(1, 128, 4, 1) EB_R64(2, 256, 2, 3) EB_R64(3, 128, 4, 3) default: break; }
   } else {
@@ -1419,7 +1423,7 @@ int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* nu
       if (desc) {
         desc[12 * kind + 3 * i] = sh.nt;
         desc[12 * kind + 3 * i + 1] = sh.tpt;
-        desc[12 * kind + 3 * i + 2] = sh.rcp;
+        desc[12 * kind + 3 * i + 2] = sh.rcp + 10 * sh.minb;   // FP32: unroll + 10 x resident CTAs
       }
       if (ms) ms[8 * kind + i] = s.tune_ms[kind][i] < 1e29f ? s.tune_ms[kind][i] : 0.f;
     }

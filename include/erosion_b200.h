@@ -447,7 +447,8 @@ int erosion_set_far_shape(int32_t kind, int32_t shape);
  * is, for the FP64 kernels, the reciprocal: 1 FP32 estimate + 2
  * Newton-Raphson steps, 3 FP64 estimate + 2 steps (accurate kind), 2 FP32
  * estimate + 1 step, 4 FP64 estimate + 1 step (fast kind); for the FP32
- * kernel the unroll factor of the source loop.  ms[8*kind + i] = the
+ * kernel the unroll factor of the source loop plus 10 x the resident CTAs
+ * per SM it is compiled for (its register budget).  ms[8*kind + i] = the
  * autotuner's time of candidate i in milliseconds (0 when not timed;
  * capacity 24).  Any pointer may be NULL. */
 int erosion_get_far_shapes(int32_t* shape, int32_t* desc, float* ms, int32_t* num_shapes);
