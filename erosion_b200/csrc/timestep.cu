@@ -111,8 +111,9 @@ __global__ void k_lw_delta(long long n, const double* __restrict__ x, double* __
 // double-layer block, so its size (~6e5 for the smallest bodies of a dense
 // packing) is set by the stokeslet/rotlet rows alone, while the nodes slide
 // along the curves between solves (the theta-L update keeps them at equal
-// arclength): index-aligned, that rigid part leaves a residual of ~1e3 ||b||;
-// carried to the new nodes, ~1e-2 ||b||.  Nodes are at equal arclength, so
+// arclength): index-aligned, that rigid part leaves a residual of ~1e3 ||b||
+// (200 bodies); carried to the new nodes, 2e-2 ||b|| (10 bodies, dt 1e-5) to
+// 0.3 ||b|| (200 bodies, dt 2e-6).  Nodes are at equal arclength, so
 // node means are arclength means.  Wall and stokeslet/rotlet entries are
 // copied unchanged.
 __global__ void __launch_bounds__(TL_NT)
