@@ -600,7 +600,13 @@ static void solve_wall_rows(State& s, const double* d_r, double* d_c) {
   EB_CK(cudaMemsetAsync(dx, 0, nw * sizeof(double), w.st));
   long long it = 0;
   double est = 0;
-  const int rc = gmres_solve(w, rb, dx, true, 200, 1e-6, &it, &est);
+  int rc = EROSION_OK;
+  try {
+    rc = gmres_solve(w, rb, dx, true, 200, 1e-6, &it, &est);
+  } catch (const Error& e) {
+    if (e.code != EROSION_BAD_INPUT) throw;   // a zero wall residual: nothing to add
+    return;
+  }
   if (rc == EROSION_BREAKDOWN) return;   // leave the candidate's wall part as it is
   k_axpy<<<nblk(nw, 256), 256, 0, w.st>>>(1.0, dx, d_c, nw);
   EB_LAUNCH_CHECK();
