@@ -92,7 +92,7 @@ typedef struct {
   int32_t ibary;        /* 1 barycentric near field, 0 trapezoid                   */
   int32_t ifmm;         /* with ibary=1: 1 fmmbary selection rules, 0 all pairs    */
   int32_t ibc;          /* 0 parabolic, 1 uniform wall velocity                    */
-  int32_t precision;    /* 0 FP64; 1 mixed: FP32 compensated far field inside FP64
+  int32_t precision;    /* 0 FP64; 1 mixed: FP32 far field (FP64 accumulation) inside FP64
                            iterative refinement to the same tol                    */
   int32_t rhs_mode;     /* 0 production data; 1 the reference's manufactured
                            stokeslet (1,2) + rotlet 3 at the origin (:220-257);

@@ -1,4 +1,4 @@
-"""Mixed precision: the FP32 compensated far field inside FP64 iterative
+"""Mixed precision: the FP32 far field (FP64 accumulation) inside FP64 iterative
 refinement reaches the same 1e-8 relative residual as the FP64 path, and its
 density and shear stress agree with the FP64 oracle within the tolerances the
 1e-8 stopping point allows (1e-6 density, 1e-7 shear stress, relative)."""
