@@ -998,24 +998,23 @@ k_gj_inv32_blocked(int m, int pb, float* __restrict__ B, int* __restrict__ bad) 
 }
 
 // z_b = B_b^{-1} t_b for every body.  t is gathered from v (the body part of
-// the unknown vector) plus the wall coupling tw (per body node, FP64, already
-// the product A_bw z_wall); z is scattered into the same layout.  CTA = (body,
-// 256-row chunk), warp per row.
+// the unknown vector) less the wall coupling A_bw z_wall, given as ntw
+// partial sums per body node (slot q at tw + q * tw_stride, body-major); z is
+// scattered into the same layout.  CTA = (body, 256-row chunk), warp per row.
 __global__ void __launch_bounds__(256)
 k_pc_apply_bodies(GeoDev G, const float* __restrict__ Binv, const double* __restrict__ v,
-                  const double2* __restrict__ tw, int ntw, double* __restrict__ z) {
+                  const double2* __restrict__ tw, long long tw_stride, int ntw, double* __restrict__ z) {
   extern __shared__ float tv[];   // m entries of t_b
   const int b = blockIdx.x, n = G.n, m = 2 * n + 3;
   const long long sb = 2LL * G.nout + 2LL * n * b;      // sigma block of body b
   const long long cbk = 2LL * G.nout + 2LL * n * G.M + 3LL * b;
-  const size_t nb = (size_t)n * G.M;
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     double t;
     if (r < 2 * n) {
       const int k = r < n ? r : r - n;
       double cpl = 0.0;
       for (int q = 0; q < ntw; ++q) {
-        const double2 v2 = tw[q * nb + (size_t)b * n + k];
+        const double2 v2 = tw[q * tw_stride + (size_t)b * n + k];
         cpl += r < n ? v2.x : v2.y;
       }
       t = v[sb + r] - cpl;
@@ -1038,78 +1037,16 @@ k_pc_apply_bodies(GeoDev G, const float* __restrict__ Binv, const double* __rest
   }
 }
 
-// z_wall = -2 v_wall, and the FP32 source strengths w * z_wall of the wall
-// for the coupling sum.
-__global__ void k_pc_wall(GeoDev G, const double* __restrict__ v, double* __restrict__ z, float2* __restrict__ ws32) {
+// z_wall = -2 v_wall, and the FP32 source tensors of w * z_wall on the wall
+// (pair_tensor32) for the coupling sum.
+__global__ void k_pc_wall(GeoDev G, const double* __restrict__ v, double* __restrict__ z, float4* __restrict__ sq32) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.nout) return;
   const double zx = -2.0 * v[g], zy = -2.0 * v[G.nout + g];
   z[g] = zx;
   z[G.nout + g] = zy;
   const double w = G.w[g];
-  ws32[g] = make_float2((float)(w * zx), (float)(w * zy));
-}
-
-// A_bw z_wall: the wall's trapezoid double layer at every body node, FP32
-// with the same tile-relative coordinates as k_far32.  Two body nodes per
-// thread; blockIdx.y selects a contiguous range of wall tiles and writes its
-// partial sums to out[y*nb + i] (added in order by k_pc_apply_bodies).
-__global__ void __launch_bounds__(256)
-k_pc_wall2body(int nout, int nb, const float4* __restrict__ src, const float2* __restrict__ tgt,
-               const double2* __restrict__ anchor, const double2* __restrict__ tile_c, const float2* __restrict__ ws32,
-               const int4* __restrict__ tiles, int nwall_tiles, double2* __restrict__ out) {
-  __shared__ float4 sg[WALL_TS];
-  __shared__ float2 sw[WALL_TS];
-  const int tb = (int)((long long)blockIdx.y * nwall_tiles / gridDim.y);
-  const int te = (int)((long long)(blockIdx.y + 1) * nwall_tiles / gridDim.y);
-  float ox[2], oy[2], hx[2], lx[2], hy[2], ly[2];
-  double ax[2], ay[2];
-  int ii[2];
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    int i = blockIdx.x * 512 + q * 256 + threadIdx.x;
-    ii[q] = i;
-    int g = nout + (i < nb ? i : nb - 1);
-    float2 o = tgt[g];
-    double2 a = anchor[g];
-    ox[q] = o.x; oy[q] = o.y; ax[q] = a.x; ay[q] = a.y;
-    hx[q] = lx[q] = hy[q] = ly[q] = 0.f;
-  }
-  for (int ti = tb; ti < te; ++ti) {
-    const int4 T = tiles[ti];
-    __syncthreads();
-    if (threadIdx.x < T.y) { sg[threadIdx.x] = src[T.x + threadIdx.x]; sw[threadIdx.x] = ws32[T.x + threadIdx.x]; }
-    __syncthreads();
-    const double2 cs = tile_c[ti];
-    float px[2], py[2], tx[2], ty[2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      px[q] = (float)(ax[q] - cs.x) + ox[q];
-      py[q] = (float)(ay[q] - cs.y) + oy[q];
-      tx[q] = ty[q] = 0.f;
-    }
-    for (int j = 0; j < T.y; ++j) {
-      const float4 s = sg[j];
-      const float2 w = sw[j];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        float rx = px[q] - s.x, ry = py[q] - s.y;
-        float rho2 = fmaf(rx, rx, ry * ry);
-        float rdn = fmaf(rx, s.z, ry * s.w);
-        float rds = fmaf(rx, w.x, ry * w.y);
-        float inv = rcp_approx(rho2);
-        float c = (rdn * rds) * (inv * inv);
-        tx[q] = fmaf(c, rx, tx[q]);
-        ty[q] = fmaf(c, ry, ty[q]);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 2; ++q) { two_sum_add(hx[q], lx[q], tx[q]); two_sum_add(hy[q], ly[q], ty[q]); }
-  }
-#pragma unroll
-  for (int q = 0; q < 2; ++q)
-    if (ii[q] < nb)
-      out[(size_t)blockIdx.y * nb + ii[q]] = make_double2((double)hx[q] + (double)lx[q], (double)hy[q] + (double)ly[q]);
+  sq32[g] = pair_tensor32(G.nrm[g], make_double2(w * zx, w * zy));
 }
 
 // ---------------------------------------------------------------------------

@@ -354,6 +354,31 @@ static void launch_far(State& s, int kind, int shape, const int* sp, int nsplit,
   EB_LAUNCH_CHECK();
 }
 
+// The FP32 far-field kernel (the shape in use, no near mask) on the source
+// tensors sq over the tile splits sp[0..nsplit]: the preconditioner's
+// wall-to-body coupling, a far-field sum with the wall tiles as the only
+// sources.
+static void launch_far32_unmasked(State& s, const float4* sq, const int* sp, int nsplit, double2* out) {
+  const Problem& pr = s.pr;
+  cudaStream_t st = s.st;
+  const int shape = s.far_shape[1];
+  const dim3 g((unsigned)nblk(pr.N, shape_targets(1, shape)), (unsigned)nsplit);
+#define EB_FAR32U(IDX, NT, TPT, U, MB)                                                                       \
+  case IDX:                                                                                                 \
+    k_far32<false, NT, TPT, U, MB><<<g, NT, 0, st>>>(pr.N, pr.nout, pr.n, s.src32.p, s.tgt32.p, s.anchor.p,  \
+                                                  s.tile_c.p, sq, s.tiles.p, sp, nullptr, 0, out);        \
+    break;
+  switch (shape) {
+    EB_FAR32U(0, 256, 4, 2, 2)
+    EB_FAR32U(1, 256, 4, 4, 2)
+    EB_FAR32U(2, 256, 4, 2, 3)
+    EB_FAR32U(3, 256, 4, 4, 3)
+    default: throw Error(EROSION_BAD_INPUT, "unknown FP32 far-field shape");
+  }
+#undef EB_FAR32U
+  EB_LAUNCH_CHECK();
+}
+
 // Resident CTAs per SM of one far-field kernel instance (the occupancy the
 // split count is sized for); 0 when the runtime cannot tell.
 static int far_resident(int kind, int shape, bool masked) {
@@ -669,6 +694,16 @@ void setup_preconditioner(State& s) {
     return;
   }
   const int n = pr.n, m = 2 * n + 3;
+  // the wall-to-body coupling runs the FP32 far-field kernel over the wall
+  // tiles: its tile splits (whole waves, as the far field's own) and its
+  // partial sums, one N-long slot per split
+  {
+    const int sh = s.far_shape[1];
+    s.pc_wsplit = far_split_count(pr.N, s.nwall_tiles, shape_targets(1, sh), far_resident(1, sh, false));
+    upload_splits(s, s.pc_split_ptr, s.pc_wsplit, 0, s.nwall_tiles);
+    s.pc_tw.ensure((size_t)s.pc_wsplit * pr.N);
+    s.pc_sq32.ensure(pr.nout);
+  }
   // keep the previous inverses (a lagged preconditioner) when allowed
   if (pr.P.precond_refresh > 1 && s.pc_valid && s.pc_M == pr.M && s.pc_n == n && s.pc_nout == pr.nout &&
       s.pc_age + 1 < pr.P.precond_refresh) {
@@ -718,12 +753,6 @@ void setup_preconditioner(State& s) {
   for (int b = 0; b < pr.M; ++b) s.pc_singular += hbad[b] != 0;
   s.pc_z.ensure(pr.ntot);
   s.pc_u.ensure(pr.ntot);
-  {
-    const int tblk = (int)nblk((long long)pr.M * n, 512);
-    s.pc_wsplit = std::max(1, std::min(s.nwall_tiles, (4 * g_num_sms + tblk - 1) / tblk));
-  }
-  s.pc_tw.ensure((size_t)s.pc_wsplit * pr.M * n);
-  s.pc_ws32.ensure(pr.nout);
   s.pc_active = s.pc_singular < pr.M;
   s.pc_valid = true;
   s.pc_M = pr.M;
@@ -736,14 +765,11 @@ void apply_preconditioner(State& s, const double* v, double* z) {
   const Problem& pr = s.pr;
   const GeoDev G = s.geo();
   const int n = pr.n, m = 2 * n + 3, nb = n * pr.M;
-  k_pc_wall<<<nblk(pr.nout, 256), 256, 0, s.st>>>(G, v, z, s.pc_ws32.p);
+  k_pc_wall<<<nblk(pr.nout, 256), 256, 0, s.st>>>(G, v, z, s.pc_sq32.p);
   EB_LAUNCH_CHECK();
-  k_pc_wall2body<<<dim3(nblk(nb, 512), s.pc_wsplit), 256, 0, s.st>>>(pr.nout, nb, s.src32.p, s.tgt32.p, s.anchor.p,
-                                                                     s.tile_c.p, s.pc_ws32.p, s.tiles.p,
-                                                                     s.nwall_tiles, s.pc_tw.p);
-  EB_LAUNCH_CHECK();
+  launch_far32_unmasked(s, s.pc_sq32.p, s.pc_split_ptr.p, s.pc_wsplit, s.pc_tw.p);
   dim3 g(pr.M, (unsigned)std::max(1, (m + 63) / 64));
-  k_pc_apply_bodies<<<g, 256, m * sizeof(float), s.st>>>(G, s.pcB.p, v, s.pc_tw.p, s.pc_wsplit, z);
+  k_pc_apply_bodies<<<g, 256, m * sizeof(float), s.st>>>(G, s.pcB.p, v, s.pc_tw.p + pr.nout, pr.N, s.pc_wsplit, z);
   EB_LAUNCH_CHECK();
 }
 
@@ -1146,7 +1172,7 @@ void release_state_buffers(State& s) {
   s.tiles.release(); s.split_ptr.release();
   s.vcap = 0;
   s.zcap = 0;
-  s.pcB.release(); s.pc_tw.release(); s.pc_ws32.release(); s.pc_bad.release();
+  s.pcB.release(); s.pc_tw.release(); s.pc_sq32.release(); s.pc_split_ptr.release(); s.pc_bad.release();
   s.pc_valid = false;
   s.src32.release(); s.sq32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
   s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();

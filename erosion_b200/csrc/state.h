@@ -151,8 +151,9 @@ struct State {
   int nwall_tiles = 0;
   DBuf<float> pcB;          // M inverse blocks of (2n+3)^2
   DBuf<double> pc_z, pc_u;  // scratch vectors
-  DBuf<double2> pc_tw;      // A_bw z_wall per body node
-  DBuf<float2> pc_ws32;     // wall strengths of the coupling sum
+  DBuf<double2> pc_tw;      // A_bw z_wall: pc_wsplit partial sums, N long each (body nodes after the wall's)
+  DBuf<float4> pc_sq32;     // wall source tensors of the coupling sum (pair_tensor32 of w z_wall)
+  DBuf<int> pc_split_ptr;   // its splits of the wall tiles
   DBuf<int> pc_bad;         // per body: 1 when its block had a zero pivot
   int pc_singular = 0;      // bodies left unpreconditioned
   bool pc_valid = false;    // pcB holds inverses of a (pc_M, pc_n) problem
