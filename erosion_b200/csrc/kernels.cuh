@@ -1037,6 +1037,222 @@ k_pc_apply_bodies(GeoDev G, const float* __restrict__ Binv, const double* __rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// Coarse correction of the block preconditioner (precond = 2).  Coarse space
+// per body b: its rigid-motion densities r1 = (1, 0), r2 = (0, 1),
+// r3 = (-(y - yc), x - xc) ((xc, yc) = G.cen[b], the node mean the
+// stokeslets/rotlets are centred on) and the unit vectors s1, s2, s3 of its
+// stokeslet/rotlet unknowns.  A r_i is non-zero only in b's stokeslet/rotlet
+// rows (a rigid motion has no double-layer field; k_prep's constraint rows:
+// -(1/n) sum sigma |z'| and -(1/n) sum (sigma_x y - sigma_y x) |z'|), and
+// A s_j is the completion field of that unknown at every node (as k_combine
+// evaluates it) plus 1 in its own row.  So with coarse coordinates (c_r, c_s)
+// the coarse operator Q^T A Q = [[0, Bm], [C, I]]: Bm = the rigid moments
+// of the completion fields over every body's nodes (dense, 3M x 3M), C = the
+// constraint rows of the rigid densities (3 x 3 per body).
+
+// The completion field at p of unit stokeslet/rotlet unknowns (l1, l2, xi)
+// centred at c, as k_combine adds it: u = F * (l1, l2, xi).
+__device__ __forceinline__ void cg_fields(double2 p, double2 c, double f[2][3]) {
+  const double rx = p.x - c.x, ry = p.y - c.y;
+  const double rho2 = rx * rx + ry * ry;
+  const double lg = log(rho2), ir = 1.0 / rho2;
+  const double k = 0.5 / EB_TWOPI;
+  f[0][0] = k * (-0.5 * lg + rx * rx * ir);
+  f[1][0] = k * (rx * ry * ir);
+  f[0][1] = k * (rx * ry * ir);
+  f[1][1] = k * (-0.5 * lg + ry * ry * ir);
+  f[0][2] = ry * ir;
+  f[1][2] = -rx * ir;
+}
+
+// q = Q^T v: per body the sums of v over its nodes against r1, r2, r3, then
+// its three stokeslet/rotlet entries.  One CTA per body.
+__global__ void __launch_bounds__(256) k_cg_restrict(GeoDev G, const double* __restrict__ v, double* __restrict__ q) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x;
+  const double2 c = G.cen[b];
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int k = threadIdx.x; k < G.n; k += blockDim.x) {
+    const int g = G.nout + b * G.n + k;
+    const double2 p = G.xy[g];
+    const double vx = v[ix_of(G, g)], vy = v[iy_of(G, g)];
+    a0 += vx;
+    a1 += vy;
+    a2 += -(p.y - c.y) * vx + (p.x - c.x) * vy;
+  }
+  a0 = block_sum<256>(a0, sh);
+  a1 = block_sum<256>(a1, sh);
+  a2 = block_sum<256>(a2, sh);
+  if (threadIdx.x == 0) {
+    q[6 * b] = a0;
+    q[6 * b + 1] = a1;
+    q[6 * b + 2] = a2;
+    q[6 * b + 3] = v[ic_of(G, b, 0)];
+    q[6 * b + 4] = v[ic_of(G, b, 1)];
+    q[6 * b + 5] = v[ic_of(G, b, 2)];
+  }
+}
+
+// Bm[(3b + i) * 3M + 3k + j] = r_i^T (field of s_j of body k) over body b's
+// nodes, FP32.  CTA = (b, k).
+__global__ void __launch_bounds__(128) k_cg_moments(GeoDev G, float* __restrict__ Bm) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x, kb = blockIdx.y, M3 = 3 * G.M;
+  const double2 cb = G.cen[b], ck = G.cen[kb];
+  double m[3][3] = {};
+  for (int k = threadIdx.x; k < G.n; k += blockDim.x) {
+    const double2 p = G.xy[G.nout + b * G.n + k];
+    double f[2][3];
+    cg_fields(p, ck, f);
+    const double ex = -(p.y - cb.y), ey = p.x - cb.x;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      m[0][j] += f[0][j];
+      m[1][j] += f[1][j];
+      m[2][j] += ex * f[0][j] + ey * f[1][j];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double t = block_sum<128>(m[i][j], sh);
+      if (threadIdx.x == 0) Bm[(size_t)(3 * b + i) * M3 + 3 * kb + j] = (float)t;
+    }
+}
+
+// Cinv (9 per body, FP64): the inverse of C_b, C_b[row][col] = constraint
+// row `row` of A applied to r_col (the rows k_prep writes: -(1/n) sum of
+// sigma_x |z'|, of sigma_y |z'|, of (sigma_x y - sigma_y x) |z'|).  A
+// singular C_b (not expected for a closed curve) gets the zero inverse.
+__global__ void __launch_bounds__(256) k_cg_constraints(GeoDev G, double* __restrict__ Cinv) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x;
+  const double2 c = G.cen[b];
+  double s0 = 0, sx = 0, sy = 0, sxe = 0, sye = 0, sr = 0;
+  for (int k = threadIdx.x; k < G.n; k += blockDim.x) {
+    const int g = G.nout + b * G.n + k;
+    const double2 p = G.xy[g];
+    const double w = G.sp[g];
+    s0 += w;
+    sx += p.x * w;
+    sy += p.y * w;
+    sxe += (p.x - c.x) * w;
+    sye += (p.y - c.y) * w;
+    sr += ((p.y - c.y) * p.y + (p.x - c.x) * p.x) * w;
+  }
+  s0 = block_sum<256>(s0, sh);
+  sx = block_sum<256>(sx, sh);
+  sy = block_sum<256>(sy, sh);
+  sxe = block_sum<256>(sxe, sh);
+  sye = block_sum<256>(sye, sh);
+  sr = block_sum<256>(sr, sh);
+  if (threadIdx.x != 0) return;
+  const double n = G.n;
+  // columns: A r1, A r2, A r3 in the three constraint rows
+  double C[3][3] = {{-s0 / n, 0.0, sye / n}, {0.0, -s0 / n, -sxe / n}, {-sy / n, sx / n, sr / n}};
+  const double det = C[0][0] * (C[1][1] * C[2][2] - C[1][2] * C[2][1]) -
+                     C[0][1] * (C[1][0] * C[2][2] - C[1][2] * C[2][0]) +
+                     C[0][2] * (C[1][0] * C[2][1] - C[1][1] * C[2][0]);
+  double* o = Cinv + 9 * b;
+  if (!(fabs(det) > 0.0)) {
+    for (int i = 0; i < 9; ++i) o[i] = 0.0;
+    return;
+  }
+  const double id = 1.0 / det;
+  o[0] = (C[1][1] * C[2][2] - C[1][2] * C[2][1]) * id;
+  o[1] = (C[0][2] * C[2][1] - C[0][1] * C[2][2]) * id;
+  o[2] = (C[0][1] * C[1][2] - C[0][2] * C[1][1]) * id;
+  o[3] = (C[1][2] * C[2][0] - C[1][0] * C[2][2]) * id;
+  o[4] = (C[0][0] * C[2][2] - C[0][2] * C[2][0]) * id;
+  o[5] = (C[0][2] * C[1][0] - C[0][0] * C[1][2]) * id;
+  o[6] = (C[1][0] * C[2][1] - C[1][1] * C[2][0]) * id;
+  o[7] = (C[0][1] * C[2][0] - C[0][0] * C[2][1]) * id;
+  o[8] = (C[0][0] * C[1][1] - C[0][1] * C[1][0]) * id;
+}
+
+// Coarse solve, stokeslet/rotlet part: c_s = Bm^{-1} q_r (one warp per row
+// of the FP32 inverse, FP64 accumulation).  cs[3b + j].
+__global__ void __launch_bounds__(256) k_cg_solve_s(int M, const float* __restrict__ Binv,
+                                                    const double* __restrict__ q, double* __restrict__ cs) {
+  const int M3 = 3 * M;
+  const int row = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= M3) return;
+  double acc = 0.0;
+  for (int c = lane; c < M3; c += 32) acc += (double)Binv[(size_t)row * M3 + c] * q[6 * (c / 3) + (c % 3)];
+  acc = warp_sum(acc);
+  if (lane == 0) cs[row] = acc;
+}
+
+// Coarse solve, rigid part c_r = C_b^{-1} (q_s - c_s), then the coarse
+// residual update of the constraint rows: w = v - A Q c there, A Q c = C_b c_r
+// + c_s (the rigid densities' constraint rows and the unknowns' own 1).
+// One thread per body.  cr[3b + i].
+__global__ void k_cg_solve_r(GeoDev G, const double* __restrict__ Cinv, const double* __restrict__ q,
+                             const double* __restrict__ cs, double* __restrict__ cr, double* __restrict__ w) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= G.M) return;
+  const double* Ci = Cinv + 9 * b;
+  double t[3], r[3];
+  for (int i = 0; i < 3; ++i) t[i] = q[6 * b + 3 + i] - cs[3 * b + i];
+  for (int i = 0; i < 3; ++i) r[i] = Ci[3 * i] * t[0] + Ci[3 * i + 1] * t[1] + Ci[3 * i + 2] * t[2];
+  for (int i = 0; i < 3; ++i) cr[3 * b + i] = r[i];
+  // C_b r = t exactly when C_b is regular, so the constraint rows of A Q c
+  // are t + c_s = q_s; the zero inverse (singular C_b) leaves c_r = 0
+  const bool reg = Ci[0] != 0.0 || Ci[4] != 0.0 || Ci[8] != 0.0;
+  for (int i = 0; i < 3; ++i) w[ic_of(G, b, i)] -= (reg ? t[i] : 0.0) + cs[3 * b + i];
+}
+
+// The density rows of w = v - A Q c: minus the completion field of c_s at
+// every node (wall and bodies).  One thread per node, the centres staged in
+// shared memory.
+__global__ void __launch_bounds__(256) k_cg_field(GeoDev G, const double* __restrict__ cs, double* __restrict__ w) {
+  __shared__ double4 sc[256];   // cx, cy, l1, l2
+  __shared__ double sxi[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < G.N;
+  const double2 p = G.xy[act ? i : 0];
+  double ux = 0.0, uy = 0.0;
+  for (int b0 = 0; b0 < G.M; b0 += 256) {
+    __syncthreads();
+    const int t = b0 + threadIdx.x;
+    if (t < G.M) {
+      const double2 c = G.cen[t];
+      sc[threadIdx.x] = make_double4(c.x, c.y, cs[3 * t], cs[3 * t + 1]);
+      sxi[threadIdx.x] = cs[3 * t + 2];
+    }
+    __syncthreads();
+    const int nb = min(256, G.M - b0);
+    for (int j = 0; j < nb; ++j) {
+      const double4 q = sc[j];
+      double f[2][3];
+      cg_fields(p, make_double2(q.x, q.y), f);
+      ux += f[0][0] * q.z + f[0][1] * q.w + f[0][2] * sxi[j];
+      uy += f[1][0] * q.z + f[1][1] * q.w + f[1][2] * sxi[j];
+    }
+  }
+  if (!act) return;
+  w[ix_of(G, i)] -= ux;
+  w[iy_of(G, i)] -= uy;
+}
+
+// z += Q c: the rigid densities c_r on every body's nodes and c_s in its
+// stokeslet/rotlet unknowns.  One CTA per body.
+__global__ void __launch_bounds__(256) k_cg_prolong(GeoDev G, const double* __restrict__ cr,
+                                                    const double* __restrict__ cs, double* __restrict__ z) {
+  const int b = blockIdx.x;
+  const double2 c = G.cen[b];
+  const double r0 = cr[3 * b], r1 = cr[3 * b + 1], r2 = cr[3 * b + 2];
+  for (int k = threadIdx.x; k < G.n; k += blockDim.x) {
+    const int g = G.nout + b * G.n + k;
+    const double2 p = G.xy[g];
+    z[ix_of(G, g)] += r0 - r2 * (p.y - c.y);
+    z[iy_of(G, g)] += r1 + r2 * (p.x - c.x);
+  }
+  if (threadIdx.x < 3) z[ic_of(G, b, threadIdx.x)] += cs[3 * b + threadIdx.x];
+}
+
 // z_wall = -2 v_wall, and the FP32 source tensors of w * z_wall on the wall
 // (pair_tensor32) for the coupling sum.
 __global__ void k_pc_wall(GeoDev G, const double* __restrict__ v, double* __restrict__ z, float4* __restrict__ sq32) {

@@ -685,12 +685,62 @@ bool choose_initial_guess(State& s, const double* d_b, double* d_x, bool have_x,
   return used == 0;
 }
 
+// In-place inversion of count m x m FP32 matrices (one CTA each), a zero
+// pivot flagged in bad[matrix].  Blocked Gauss-Jordan with the widest panel
+// whose shared-memory working set (2 m pb + m floats, m ints) fits; the
+// unblocked kernel past that.
+static void invert_fp32(State& s, float* B, int m, int count, int* bad) {
+  int pb = 32;
+  auto gj_smem = [m](int b) { return (2 * (size_t)m * b + m) * sizeof(float) + (size_t)m * sizeof(int); };
+  while (pb > 4 && gj_smem(pb) > 200 * 1024) pb /= 2;
+  if (gj_smem(pb) <= 200 * 1024) {
+    const size_t smem = gj_smem(pb);
+    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32_blocked);
+    k_gj_inv32_blocked<<<count, 512, smem, s.st>>>(m, pb, B, bad);
+    EB_LAUNCH_CHECK();
+  } else {
+    const size_t smem = 3 * (size_t)m * sizeof(float);
+    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32);
+    k_gj_inv32<<<count, 1024, smem, s.st>>>(m, B, bad);
+    EB_LAUNCH_CHECK();
+  }
+}
+
+// The coarse correction of precond = 2 (kernels.cuh, k_cg_*): the constraint
+// rows' 3 x 3 inverses and the inverse of the rigid moments of the
+// completion fields, for the current geometry.  cg_ready is false when that
+// matrix had a zero pivot (the block preconditioner then runs alone).
+static void setup_coarse(State& s) {
+  const Problem& pr = s.pr;
+  s.cg_ready = false;
+  if (pr.P.precond != 2 || pr.M == 0) return;
+  const GeoDev G = s.geo();
+  const int m3 = 3 * pr.M;
+  k_cg_constraints<<<pr.M, 256, 0, s.st>>>(G, s.cg_Cinv.ensure(9LL * pr.M));
+  EB_LAUNCH_CHECK();
+  float* Bm = s.cg_B.ensure((size_t)m3 * m3);
+  k_cg_moments<<<dim3(pr.M, pr.M), 128, 0, s.st>>>(G, Bm);
+  EB_LAUNCH_CHECK();
+  int* bad = s.cg_bad.ensure(1);
+  EB_CK(cudaMemsetAsync(bad, 0, sizeof(int), s.st));
+  invert_fp32(s, Bm, m3, 1, bad);
+  s.cg_q.ensure(6LL * pr.M);
+  s.cg_cs.ensure(3LL * pr.M);
+  s.cg_cr.ensure(3LL * pr.M);
+  s.pc_u.ensure(pr.ntot);
+  int hbad = 0;
+  d2h(&hbad, bad, 1, s.st);
+  EB_CK(cudaStreamSynchronize(s.st));
+  s.cg_ready = hbad == 0;
+}
+
 void setup_preconditioner(State& s) {
   const Problem& pr = s.pr;
   s.pc_setup_ms = 0.0;
-  if (pr.P.precond != 1 || pr.M == 0) {
+  if ((pr.P.precond != 1 && pr.P.precond != 2) || pr.M == 0) {
     s.pc_active = false;
     s.pc_singular = 0;
+    s.cg_ready = false;
     return;
   }
   const int n = pr.n, m = 2 * n + 3;
@@ -709,6 +759,7 @@ void setup_preconditioner(State& s) {
       s.pc_age + 1 < pr.P.precond_refresh) {
     s.pc_age++;
     s.pc_active = s.pc_singular < pr.M;
+    setup_coarse(s);
     return;
   }
   s.pc_active = false;
@@ -721,22 +772,7 @@ void setup_preconditioner(State& s) {
   EB_LAUNCH_CHECK();
   int* bad = s.pc_bad.ensure(pr.M);
   EB_CK(cudaMemsetAsync(bad, 0, sizeof(int) * pr.M, s.st));
-  // blocked Gauss-Jordan: the widest panel whose shared-memory working set
-  // (2 m pb + m floats, m ints) fits; the unblocked kernel past that
-  int pb = 32;
-  auto gj_smem = [m](int b) { return (2 * (size_t)m * b + m) * sizeof(float) + (size_t)m * sizeof(int); };
-  while (pb > 4 && gj_smem(pb) > 200 * 1024) pb /= 2;
-  if (gj_smem(pb) <= 200 * 1024) {
-    const size_t smem = gj_smem(pb);
-    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32_blocked);
-    k_gj_inv32_blocked<<<pr.M, 512, smem, s.st>>>(m, pb, B, bad);
-    EB_LAUNCH_CHECK();
-  } else {
-    const size_t smem = 3 * (size_t)m * sizeof(float);
-    if (smem > 48 * 1024) allow_max_dynamic_smem((const void*)k_gj_inv32);
-    k_gj_inv32<<<pr.M, 1024, smem, s.st>>>(m, B, bad);
-    EB_LAUNCH_CHECK();
-  }
+  invert_fp32(s, B, m, pr.M, bad);
   // a body whose block had a zero pivot gets the identity (left
   // unpreconditioned); the other bodies keep their inverses
   k_pc_identity_if_bad<<<dim3(pr.M, nblk(m, 8)), 256, 0, s.st>>>(m, bad, B);
@@ -753,6 +789,7 @@ void setup_preconditioner(State& s) {
   for (int b = 0; b < pr.M; ++b) s.pc_singular += hbad[b] != 0;
   s.pc_z.ensure(pr.ntot);
   s.pc_u.ensure(pr.ntot);
+  setup_coarse(s);
   s.pc_active = s.pc_singular < pr.M;
   s.pc_valid = true;
   s.pc_M = pr.M;
@@ -761,7 +798,34 @@ void setup_preconditioner(State& s) {
   s.pc_age = 0;
 }
 
+static void apply_block_gs(State& s, const double* v, double* z);
+
+// precond = 1: block Gauss-Seidel.  precond = 2: first the coarse problem
+// Q^T A Q c = Q^T v (k_cg_*), then block Gauss-Seidel on the rest,
+// z = Q c + P (v - A Q c).
 void apply_preconditioner(State& s, const double* v, double* z) {
+  const Problem& pr = s.pr;
+  if (pr.P.precond != 2 || !s.cg_ready) {
+    apply_block_gs(s, v, z);
+    return;
+  }
+  const GeoDev G = s.geo();
+  double* w = s.pc_u.p;
+  EB_CK(cudaMemcpyAsync(w, v, pr.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+  k_cg_restrict<<<pr.M, 256, 0, s.st>>>(G, v, s.cg_q.p);
+  EB_LAUNCH_CHECK();
+  k_cg_solve_s<<<(unsigned)nblk(3LL * pr.M, 8), 256, 0, s.st>>>(pr.M, s.cg_B.p, s.cg_q.p, s.cg_cs.p);
+  EB_LAUNCH_CHECK();
+  k_cg_solve_r<<<(unsigned)nblk(pr.M, 128), 128, 0, s.st>>>(G, s.cg_Cinv.p, s.cg_q.p, s.cg_cs.p, s.cg_cr.p, w);
+  EB_LAUNCH_CHECK();
+  k_cg_field<<<(unsigned)nblk(pr.N, 256), 256, 0, s.st>>>(G, s.cg_cs.p, w);
+  EB_LAUNCH_CHECK();
+  apply_block_gs(s, w, z);
+  k_cg_prolong<<<pr.M, 256, 0, s.st>>>(G, s.cg_cr.p, s.cg_cs.p, z);
+  EB_LAUNCH_CHECK();
+}
+
+static void apply_block_gs(State& s, const double* v, double* z) {
   const Problem& pr = s.pr;
   const GeoDev G = s.geo();
   const int n = pr.n, m = 2 * n + 3, nb = n * pr.M;
@@ -1173,6 +1237,8 @@ void release_state_buffers(State& s) {
   s.vcap = 0;
   s.zcap = 0;
   s.pcB.release(); s.pc_tw.release(); s.pc_sq32.release(); s.pc_split_ptr.release(); s.pc_bad.release();
+  s.cg_B.release(); s.cg_Cinv.release(); s.cg_q.release(); s.cg_cs.release(); s.cg_cr.release(); s.cg_bad.release();
+  s.cg_ready = false;
   s.pc_valid = false;
   s.src32.release(); s.sq32.release(); s.tgt32.release(); s.tile_c.release(); s.anchor.release();
   s.self_tasks.release(); s.selfsum.release(); s.split_ptr32.release(); s.split_ptr64t.release(); s.split_ptrw.release();

@@ -154,6 +154,13 @@ struct State {
   DBuf<double2> pc_tw;      // A_bw z_wall: pc_wsplit partial sums, N long each (body nodes after the wall's)
   DBuf<float4> pc_sq32;     // wall source tensors of the coupling sum (pair_tensor32 of w z_wall)
   DBuf<int> pc_split_ptr;   // its splits of the wall tiles
+  // coarse correction (precond = 2): inverse of the completion fields' rigid
+  // moments (3M x 3M, FP32), the constraint rows' 3 x 3 inverses (FP64),
+  // coarse coordinates
+  DBuf<float> cg_B;
+  DBuf<double> cg_Cinv, cg_q, cg_cs, cg_cr;
+  DBuf<int> cg_bad;
+  bool cg_ready = false;
   DBuf<int> pc_bad;         // per body: 1 when its block had a zero pivot
   int pc_singular = 0;      // bodies left unpreconditioned
   bool pc_valid = false;    // pcB holds inverses of a (pc_M, pc_n) problem

@@ -90,3 +90,18 @@ def test_fp32_from_the_first_iteration_with_decade_sweeps(lib, oracle, name):
     tau, _ = stokes.shear_stress(g, den)
     tau_o, _ = oracle.shear_stress(g, ref)
     assert rel(tau, tau_o) < 1e-7
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_coarse_correction_same_answer_fewer_iterations(lib, oracle, precision):
+    """precond = 2 (block Gauss-Seidel after a coarse correction on every
+    body's rigid-motion densities and stokeslet/rotlet unknowns) reaches the
+    same tolerance and the oracle's density in no more iterations than the
+    block preconditioner alone."""
+    g = G.workload("c1", seed=4)
+    _, n1, _ = stokes.solve(g, precision=precision, precond=1)
+    den, n2, st = stokes.solve(g, precision=precision, precond=2, true_residual=1)
+    assert st["true_residual"] <= 2e-8 and st["precond_active"] == 1
+    assert n2 <= n1
+    ref, _, _, _ = oracle.solve(g, tol=1e-13)
+    assert np.linalg.norm(den - ref) / np.linalg.norm(ref) < 1e-6
