@@ -103,8 +103,10 @@ typedef struct {
                            -2 I, wall-to-body coupling, exact inverse of every
                            body's (2 npts + 3) block in FP32; 2: as 1 after a
                            coarse correction on every body's rigid-motion
-                           densities and stokeslet/rotlet unknowns.  The stopping
-                           test is unchanged: ||b - A x||/||b|| <= tol              */
+                           densities and stokeslet/rotlet unknowns (fewer
+                           iterations at 10-30 bodies, many more at 100-400:
+                           experimental).  The stopping test is unchanged:
+                           ||b - A x||/||b|| <= tol                                 */
   int32_t learned_guess; /* 1: also try the learned initial guess (the network of
                            erosion_lw_train) and start GMRES from whichever of
                            {learned, supplied density, zero} has the smallest FP64
